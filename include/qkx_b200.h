@@ -1,0 +1,242 @@
+/*
+ * qkx_b200.h -- C ABI of the B200 twisted-mass Dslash / CG library
+ * (libqkx_b200.so).  Plain pointers and sizes only.
+ *
+ * It replaces the hot path of khadjiyiannakou/qkxTM_MPI: the operators that
+ * are member functions of qkxTM::Vector (include/lattice_util.h:80-156), the
+ * CG solver (include/solvers.h:3-22) and the qkxTM BLAS
+ * (include/blas_qkxTM.h:3-5).  Each declaration names the reference
+ * interface it stands in for.
+ *
+ * Host field layouts are the reference's own (so a caller hands over
+ * Vector::M / Gauge::M unchanged):
+ *   spinor  double[V][4][3][2]     (Vector::M,  include/lattice_util.h:90)
+ *   gauge   double[V][4][3][3][2]  (Gauge::M,   include/lattice_util.h:198)
+ *   site    x + Lx*(y + Ly*(z + Lz*t))  (LEXIC, include/qkxTM.h:130)
+ * Device-resident fields (the *_dev entry points) use the library's even-odd
+ * layout: double2 [parity][12][V/2], parity = (x+y+z+t)&1, site within a
+ * parity = lexicographic index / 2.  qkx_spinor_bytes() gives the size.
+ *
+ * Errors: every call returns an int status (QKX_OK = 0, negative on error)
+ * where the reference aborted the MPI job (errorQKXTM, include/qkxTM.h:137).
+ * qkx_last_error() returns a message for the calling thread.
+ * A context is not thread-safe; use one per thread.  All work of a context
+ * runs on its own CUDA stream; calls that take host buffers return after the
+ * results are in host memory.  The *_dev entry points are asynchronous on
+ * that stream (qkx_sync waits).
+ *
+ * Lx must be even (the even-odd layout pairs x and x+1).
+ */
+#ifndef QKX_B200_H
+#define QKX_B200_H
+
+#include <stddef.h>
+
+#if defined(__GNUC__)
+#define QKX_API __attribute__((visibility("default")))
+#else
+#define QKX_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define QKX_OK 0
+#define QKX_ERR_INVALID (-1)        /* bad argument: null pointer, size, enum value */
+#define QKX_ERR_CUDA (-2)           /* a CUDA call failed */
+#define QKX_ERR_NOMEM (-3)          /* device or pinned allocation failed */
+#define QKX_ERR_NOGAUGE (-4)        /* operator used before qkx_load_gauge */
+#define QKX_ERR_NOT_CONVERGED (-5)  /* solver stopped at maxIter; the iterate is still written */
+#define QKX_ERR_NAN (-6)            /* a solver scalar became NaN or Inf */
+#define QKX_ERR_UNSUPPORTED (-7)    /* e.g. 12-real links requested for non-SU(3) links */
+
+/* Mirrors the hot-path fields of struct LatticeInfo (include/qkxTM.h:156-204).
+ * The process grid P is absent: one GPU holds the whole lattice. */
+typedef struct qkx_params {
+  int L[4];             /* LatticeInfo::L, x y z t */
+  double kappa;         /* LatticeInfo::kappa */
+  double mu;            /* LatticeInfo::mu */
+  int twistSign;        /* LatticeInfo::twistSign, +1 or -1 */
+  int boundaryT;        /* LatticeInfo::boundaryT, +1 periodic, -1 antiperiodic */
+  double tol;           /* LatticeInfo::tol */
+  int maxIter;          /* LatticeInfo::maxIter */
+  double reliableDelta; /* LatticeInfo::reliableDelta (used by the mixed-precision solvers) */
+} qkx_params;
+
+typedef struct qkx_ctx qkx_ctx;
+
+/* Library version string. */
+QKX_API const char* qkx_version(void);
+/* Message of the last failing call on this thread ("" if none). */
+QKX_API const char* qkx_last_error(void);
+
+/* Create a context on a CUDA device: allocates the device work fields for the
+ * lattice L.  Replaces the construction of LatticeGeometry / Vector / Gauge
+ * (lib/lattice_util.cpp:44-380) for the hot path. */
+QKX_API int qkx_create(const qkx_params* p, int device, qkx_ctx** out);
+QKX_API void qkx_destroy(qkx_ctx* ctx);
+/* Change kappa, mu, twistSign, boundaryT, tol, maxIter, reliableDelta
+ * (L must stay the same).  A changed boundaryT takes effect at the next
+ * qkx_load_gauge / qkx_gauge_generate. */
+QKX_API int qkx_set_params(qkx_ctx* ctx, const qkx_params* p);
+QKX_API int qkx_get_params(const qkx_ctx* ctx, qkx_params* p);
+/* Wait for all work queued on the context's stream. */
+QKX_API int qkx_sync(qkx_ctx* ctx);
+/* The context's cudaStream_t, as void*. */
+QKX_API void* qkx_stream(qkx_ctx* ctx);
+/* Bytes of a device spinor field in the even-odd layout (both parities). */
+QKX_API size_t qkx_spinor_bytes(const qkx_ctx* ctx);
+QKX_API size_t qkx_volume(const qkx_ctx* ctx);
+
+/* ---------------------------------------------------------------- gauge */
+/* How the links passed to qkx_load_gauge relate to the boundary condition. */
+#define QKX_LINKS_AS_GIVEN 0  /* the operator uses the links exactly as passed, like
+                                 Vector::tm does (the caller may already have run
+                                 Gauge::applyBoundaryCondition, lib/lattice_util.cpp:708) */
+#define QKX_LINKS_APPLY_BC 1  /* the operator applies boundaryT itself, as if
+                                 Gauge::applyBoundaryCondition had been called */
+
+/* Upload a gauge field in Gauge::M layout.  Replaces filling Gauge::M plus
+ * Gauge::applyBoundaryCondition (lib/lattice_util.cpp:708-724) and the halo
+ * exchange Gauge::communicateToPlus (:726-774), which has no counterpart on
+ * one GPU.  The library also builds the compressed (12-real) copies used by
+ * the mixed-precision solvers when the links are SU(3) up to a global sign on
+ * the last time slice; otherwise those solvers return QKX_ERR_UNSUPPORTED. */
+QKX_API int qkx_load_gauge(qkx_ctx* ctx, const double* U_host, int bc_mode);
+/* Generate U_mu(x) = exp(i eps H) on the device (H traceless Hermitian from
+ * unit complex Gaussians, counter-based generator keyed by seed) and use it
+ * with bc_mode as in qkx_load_gauge.  No reference counterpart: the reference
+ * reads ILDG files (lib/read_conf_lime.cpp). */
+QKX_API int qkx_gauge_generate(qkx_ctx* ctx, double eps, unsigned long long seed, int bc_mode);
+/* Download the links the operator uses (boundary sign included), Gauge::M layout. */
+QKX_API int qkx_download_gauge(qkx_ctx* ctx, double* U_host);
+/* 1 if 12-real compressed links are available, 0 if not, <0 on error. */
+QKX_API int qkx_gauge_compressible(const qkx_ctx* ctx);
+
+/* ---------------------------------------------------------------- operators */
+/* Operator ids.  Each names the reference member function it reproduces
+ * (all in lib/lattice_util.cpp); out = op(in) on full-lattice fields, with the
+ * parity the reference zero-fills written as zero. */
+enum qkx_op {
+  QKX_OP_DSLASH = 0,                  /* Vector::applyDslash                 :1158 */
+  QKX_OP_DSLASH_DAG = 1,              /* Vector::applyDslashDag              :1643 */
+  QKX_OP_TM = 2,                      /* Vector::tm                          :1925 */
+  QKX_OP_TM_DAG = 3,                  /* Vector::tmDag                       :1935 */
+  QKX_OP_TM_DAGTM = 4,                /* Vector::tmDagtm                     :1940 */
+  QKX_OP_WILSON = 5,                  /* Vector::Wilson                      :1949 */
+  QKX_OP_TM_XX_EE = 6,                /* Vector::tm_xx(.., EE)               :2001 */
+  QKX_OP_TM_XX_OO = 7,                /* Vector::tm_xx(.., OO)               :2001 */
+  QKX_OP_TM_XX_DAGTM_XX_EE = 8,       /* Vector::tm_xxDagTm_xx(.., EE)       :2024 */
+  QKX_OP_TM_XX_DAGTM_XX_OO = 9,       /* Vector::tm_xxDagTm_xx(.., OO)       :2024 */
+  QKX_OP_DSLASH_CHIRAL = 10,          /* Vector::applyDslash_chiral          :1215 */
+  QKX_OP_TM_CHIRAL = 11,              /* Vector::tm_chiral                   :1930 */
+  QKX_OP_TM_XX_CHIRAL_EE = 12,        /* Vector::tm_xx_chiral(.., EE)        :2037 */
+  QKX_OP_TM_XX_CHIRAL_OO = 13,        /* Vector::tm_xx_chiral(.., OO)        :2037 */
+  QKX_OP_TM_XX_DAGTM_XX_CHIRAL_EE = 14, /* Vector::tm_xxDagTm_xx_chiral(..EE) :2060 */
+  QKX_OP_TM_XX_DAGTM_XX_CHIRAL_OO = 15, /* Vector::tm_xxDagTm_xx_chiral(..OO) :2060 */
+  QKX_OP_GAMMA5 = 16,                 /* Vector::applyGamma5                 :1778 */
+  QKX_OP_GAMMA5_CHIRAL = 17,          /* Vector::applyGamma5_chiral          :1800 */
+  QKX_OP_TWIST = 18,                  /* Vector::applyTwist                  :1563 */
+  QKX_OP_TWIST_INV = 19,              /* Vector::applyTwistInv               :1588 */
+  QKX_OP_TWIST_DAG = 20,              /* Vector::applyTwistDag               :1726 */
+  QKX_OP_TWIST_DAG_INV = 21,          /* Vector::applyTwistDagInv            :1751 */
+  QKX_OP_TWIST_INV_CHIRAL = 22,       /* Vector::applyTwistInv_chiral        :1615 */
+  QKX_OP_DSLASH_XX_EO = 23,           /* Vector::applyDslash_xx(.., EO)      :1272 */
+  QKX_OP_DSLASH_XX_OE = 24,           /* Vector::applyDslash_xx(.., OE)      :1272 */
+  QKX_OP_ROTATE_CHIRAL_TO_UKQCD = 25, /* Vector::rotateFromChiralToUKQCD     :1834 */
+  QKX_OP_DSLASH_XX_CHIRAL_EO = 26,    /* Vector::applyDslash_xx_chiral(.., EO) :1346 */
+  QKX_OP_DSLASH_XX_CHIRAL_OE = 27,    /* Vector::applyDslash_xx_chiral(.., OE) :1346 */
+  QKX_OP_TM_DAG_CHIRAL = 28,          /* tmDag in the chiral basis (no reference member; D^+ of :1215) */
+  QKX_OP_TM_DAGTM_CHIRAL = 29,        /* tmDagtm in the chiral basis (no reference member) */
+  QKX_OP_COUNT = 30
+};
+
+/* out = op(in), host buffers in Vector::M layout.  in and out may alias. */
+QKX_API int qkx_apply(qkx_ctx* ctx, int op, const double* in_host, double* out_host);
+/* out = op(in), device fields in the even-odd layout (in != out). */
+QKX_API int qkx_apply_dev(qkx_ctx* ctx, int op, const double* in_dev, double* out_dev);
+/* Host Vector::M layout <-> device even-odd layout (both on the context stream). */
+QKX_API int qkx_spinor_upload(qkx_ctx* ctx, const double* host, double* dev);
+QKX_API int qkx_spinor_download(qkx_ctx* ctx, const double* dev, double* host);
+
+/* ---------------------------------------------------------------- BLAS */
+/* Device fields in the even-odd layout, FP64, whole lattice. */
+/* reCdotXdagY (lib/blas_qkxTM.cpp:4-28): Re sum conj(x) y */
+QKX_API int qkx_reCdotXdagY(qkx_ctx* ctx, const double* x_dev, const double* y_dev, double* result);
+/* X_eq_X_p_aY (lib/blas_qkxTM.cpp:31-42): x = x + a y */
+QKX_API int qkx_X_eq_X_p_aY(qkx_ctx* ctx, double* x_dev, double a, const double* y_dev);
+/* X_eq_aX_p_Y (lib/blas_qkxTM.cpp:45-56): x = a x + y */
+QKX_API int qkx_X_eq_aX_p_Y(qkx_ctx* ctx, double* x_dev, double a, const double* y_dev);
+/* Vector::norm2 (lib/lattice_util.cpp:464-477) */
+QKX_API int qkx_norm2(qkx_ctx* ctx, const double* x_dev, double* result);
+
+/* ---------------------------------------------------------------- solvers */
+typedef struct qkx_solve_info {
+  int iterations;          /* CG iterations (max over right-hand sides) */
+  int reliable_updates;    /* FP64 residual recomputations (mixed precision) */
+  int converged;           /* 1 if every right-hand side met its target */
+  int restarts;            /* outer restarts made to reach the true-residual target */
+  double true_residual;    /* max over RHS of ||b - M x|| / ||b||, recomputed in FP64 */
+  double normal_residual;  /* max over RHS of the final CG residual ||r|| / ||in|| */
+  double seconds;          /* device time of the solve (CUDA events) */
+} qkx_solve_info;
+
+/* CG::operator()(out, in, param) (lib/solvers.cpp:16-81), FP64, full lattice:
+ * solves M^+M out = in with the reference's algorithm and stopping rule
+ * (r2 <= tol^2 |in|^2 or maxIter).  Like the reference, the result is ADDED
+ * to the incoming content of x (callers zero it first) and the initial
+ * residual is in.  Host buffers in Vector::M layout. */
+QKX_API int qkx_cg(qkx_ctx* ctx, const double* in_host, double* x_host, qkx_solve_info* info);
+QKX_API int qkx_cg_dev(qkx_ctx* ctx, const double* in_dev, double* x_dev, qkx_solve_info* info);
+
+/* Solver methods for qkx_invert. */
+#define QKX_SOLVER_CG_FP64 0        /* plain FP64 CG on M^+M, full lattice (the reference's method) */
+#define QKX_SOLVER_CG_EO_MIXED 1    /* even-odd Schur CG, sloppy spinors/links, FP64 reliable updates */
+
+#define QKX_PREC_DOUBLE 0
+#define QKX_PREC_SINGLE 1
+#define QKX_PREC_HALF 2
+
+typedef struct qkx_solver_params {
+  int method;              /* QKX_SOLVER_* */
+  int sloppy_precision;    /* QKX_PREC_* for the inner iterations (CG_EO_MIXED) */
+  double tol;              /* target for the true residual ||b - M x|| / ||b|| */
+  int maxIter;             /* total iteration cap */
+  double reliable_delta;   /* FP64 residual recomputation when |r| < delta * max|r| */
+  int use_graphs;          /* capture the inner iterations in CUDA graphs */
+} qkx_solver_params;
+
+/* Solve M x_i = b_i for nrhs right-hand sides (host buffers, Vector::M layout),
+ * each to ||b - M x|| / ||b|| <= sp->tol recomputed in FP64.  x is overwritten
+ * (no initial guess).  This is the drop-in for the reference's solve sequence
+ * vec_in.tmDag(b) ; CG(x, vec_in) (bin/test_invert.cpp:95-117).  info receives
+ * the aggregate. */
+QKX_API int qkx_invert(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, const double* const* b_host,
+               double* const* x_host, qkx_solve_info* info);
+/* The same on device fields in the even-odd layout. */
+QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, const double* const* b_dev,
+                   double* const* x_dev, qkx_solve_info* info);
+
+/* ---------------------------------------------------------------- memory helpers */
+/* Page-locked host memory for fast transfers (cudaHostAlloc); NULL on failure. */
+QKX_API void* qkx_host_alloc(size_t bytes);
+QKX_API void qkx_host_free(void* p);
+/* Device memory on the context's device (cudaMalloc); NULL on failure. */
+QKX_API void* qkx_device_alloc(qkx_ctx* ctx, size_t bytes);
+QKX_API void qkx_device_free(qkx_ctx* ctx, void* p);
+QKX_API int qkx_memcpy_h2d(qkx_ctx* ctx, void* dst, const void* src, size_t bytes);
+QKX_API int qkx_memcpy_d2h(qkx_ctx* ctx, void* dst, const void* src, size_t bytes);
+
+/* ---------------------------------------------------------------- profiling */
+/* When enabled, every launch of the hopping kernels is bracketed by CUDA
+ * events on the context stream; qkx_profile_read returns the count and the
+ * summed device milliseconds and bytes of algorithmic traffic since the last reset. */
+QKX_API int qkx_profile_enable(qkx_ctx* ctx, int on);
+QKX_API int qkx_profile_read(qkx_ctx* ctx, long long* launches, double* ms, double* bytes);
+QKX_API int qkx_profile_reset(qkx_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

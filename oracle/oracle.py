@@ -1,0 +1,245 @@
+"""ctypes bindings for the CPU oracle (oracle/liboracle.so) and for the
+reference's own sources compiled into oracle/_ref/libqkxref.so.
+
+TEST INFRASTRUCTURE ONLY.  Imported by tests/, by ``__graft_entry__.smoke()``
+and by the CPU-baseline leg of ``bench.py`` -- always as the checker or the
+timed CPU baseline, never as part of the product path.
+
+Arrays are numpy float64 in the reference's host layouts:
+spinor ``[V, 4, 3, 2]`` (Vector::M, include/lattice_util.h:90) and gauge
+``[V, 4, 3, 3, 2]`` (Gauge::M, include/lattice_util.h:198), site order
+x fastest (LEXIC, include/qkxTM.h:130).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libqkxref.so")
+REF_SRC = "/root/reference"
+
+UKQCD, CHIRAL = 0, 1
+EO, OE, OO, EE = 0, 1, 2, 3
+
+# operator ids of ref_shim.cpp
+REF_OPS = {
+    "dslash": 0, "dslash_dag": 1, "tm": 2, "tm_dag": 3, "tm_dagtm": 4, "wilson": 5,
+    "tm_xx_ee": 6, "tm_xx_oo": 7, "tm_xx_dagtm_xx_ee": 8, "tm_xx_dagtm_xx_oo": 9,
+    "dslash_chiral": 10, "tm_chiral": 11, "tm_xx_chiral_ee": 12, "tm_xx_chiral_oo": 13,
+    "tm_xx_dagtm_xx_chiral_ee": 14, "tm_xx_dagtm_xx_chiral_oo": 15, "gamma5": 16,
+    "gamma5_chiral": 17, "twist": 18, "twist_inv": 19, "twist_dag": 20, "twist_dag_inv": 21,
+    "twist_inv_chiral": 22, "dslash_xx_eo": 23, "dslash_xx_oe": 24,
+    "rotate_chiral_to_ukqcd": 25, "dslash_xx_chiral_eo": 26, "dslash_xx_chiral_oe": 27,
+}
+
+
+class OrcParams(C.Structure):
+    _fields_ = [("L", C.c_int * 4), ("kappa", C.c_double), ("mu", C.c_double),
+                ("twistSign", C.c_int), ("boundaryT", C.c_int), ("tol", C.c_double),
+                ("maxIter", C.c_int)]
+
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _L(L):
+    return (C.c_int * 4)(*L)
+
+
+def build(ref: bool = True) -> None:
+    """Compile the oracle (and the reference build when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    if ref and os.path.isdir(os.path.join(REF_SRC, "lib")):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), f"REF={REF_SRC}"],
+                       check=True)
+
+
+_lib = None
+_ref = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(ORACLE_SO):
+            build(ref=False)
+        _lib = C.CDLL(ORACLE_SO)
+        L = _lib
+        L.orc_volume.restype = C.c_long
+        L.orc_gauge_random.argtypes = [_ip, C.c_double, C.c_ulonglong, _dp]
+        L.orc_spinor_gaussian.argtypes = [_ip, C.c_ulonglong, _dp]
+        L.orc_spinor_point.argtypes = [_ip, _ip, C.c_int, C.c_int, _dp]
+        L.orc_plaquette.argtypes = [_ip, _dp]
+        L.orc_plaquette.restype = C.c_double
+        L.orc_re_dot.restype = C.c_double
+        L.orc_re_dot.argtypes = [C.c_long, _dp, _dp]
+        L.orc_norm2.restype = C.c_double
+        L.orc_norm2.argtypes = [C.c_long, _dp]
+        L.orc_axpy.argtypes = [C.c_long, C.c_double, _dp, _dp]
+        L.orc_xpay.argtypes = [C.c_long, C.c_double, _dp, _dp]
+        L.orc_cg.restype = C.c_int
+    return _lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        _ref = C.CDLL(REF_SO)
+        _ref.ref_apply.restype = C.c_int
+        _ref.ref_apply.argtypes = [C.c_int, _ip, C.c_double, C.c_double, C.c_int, _dp, _dp, _dp]
+        _ref.ref_blas.restype = C.c_double
+        _ref.ref_blas.argtypes = [C.c_int, _ip, C.c_double, _dp, _dp]
+        _ref.ref_cg.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                _dp, _dp, _dp]
+        _ref.ref_apply_bc.argtypes = [_ip, C.c_int, _dp]
+    return _ref
+
+
+def volume(L) -> int:
+    return int(L[0]) * L[1] * L[2] * L[3]
+
+
+def params(L, kappa, mu, twistSign=1, boundaryT=-1, tol=1e-10, maxIter=1000) -> OrcParams:
+    return OrcParams(_L(L), kappa, mu, twistSign, boundaryT, tol, maxIter)
+
+
+# ---------------------------------------------------------------- inputs
+def gauge_random(L, eps, seed) -> np.ndarray:
+    U = np.empty((volume(L), 4, 3, 3, 2))
+    lib().orc_gauge_random(_L(L), eps, seed, _ptr(U))
+    return U
+
+
+def gauge_unit(L) -> np.ndarray:
+    U = np.empty((volume(L), 4, 3, 3, 2))
+    lib().orc_gauge_unit(_L(L), _ptr(U))
+    return U
+
+
+def spinor_gaussian(L, seed) -> np.ndarray:
+    v = np.empty((volume(L), 4, 3, 2))
+    lib().orc_spinor_gaussian(_L(L), seed, _ptr(v))
+    return v
+
+
+def spinor_point(L, x, spin, colour) -> np.ndarray:
+    v = np.empty((volume(L), 4, 3, 2))
+    lib().orc_spinor_point(_L(L), (C.c_int * 4)(*x), spin, colour, _ptr(v))
+    return v
+
+
+def plaquette(L, U) -> float:
+    return lib().orc_plaquette(_L(L), _ptr(U))
+
+
+def apply_bc(L, U, boundaryT=-1) -> np.ndarray:
+    U = U.copy()
+    lib().orc_apply_bc(_L(L), boundaryT, _ptr(U))
+    return U
+
+
+# ---------------------------------------------------------------- operators
+def apply(op: str, L, U, psi, kappa=0.16, mu=0.01, twistSign=1) -> np.ndarray:
+    """Oracle operator by the same names as REF_OPS."""
+    lb = lib()
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    out = np.empty_like(psi)
+    p = params(L, kappa, mu, twistSign)
+    pp = C.byref(p)
+    Lc = _L(L)
+    basis = CHIRAL if ("chiral" in op and op != "rotate_chiral_to_ukqcd") else UKQCD
+    base = op if op == "rotate_chiral_to_ukqcd" else op.replace("_chiral", "")
+    if base == "dslash":
+        lb.orc_dslash(Lc, _ptr(U), _ptr(psi), _ptr(out), 0, basis)
+    elif base == "dslash_dag":
+        lb.orc_dslash(Lc, _ptr(U), _ptr(psi), _ptr(out), 1, basis)
+    elif base in ("dslash_xx_eo", "dslash_xx_oe"):
+        lb.orc_dslash_xx(Lc, _ptr(U), _ptr(psi), _ptr(out), EO if base.endswith("eo") else OE, basis)
+    elif base == "tm":
+        lb.orc_tm(pp, _ptr(U), _ptr(psi), _ptr(out), basis)
+    elif base == "tm_dag":
+        lb.orc_tm_dag(pp, _ptr(U), _ptr(psi), _ptr(out), basis)
+    elif base == "tm_dagtm":
+        lb.orc_tm_dagtm(pp, _ptr(U), _ptr(psi), _ptr(out), basis)
+    elif base == "wilson":
+        lb.orc_wilson(pp, _ptr(U), _ptr(psi), _ptr(out))
+    elif base in ("tm_xx_ee", "tm_xx_oo"):
+        lb.orc_tm_xx(pp, _ptr(U), _ptr(psi), _ptr(out), EE if base.endswith("ee") else OO, basis)
+    elif base in ("tm_xx_dagtm_xx_ee", "tm_xx_dagtm_xx_oo"):
+        lb.orc_tm_xx_dagtm_xx(pp, _ptr(U), _ptr(psi), _ptr(out),
+                              EE if base.endswith("ee") else OO, basis)
+    elif base == "gamma5":
+        lb.orc_gamma5(Lc, _ptr(psi), _ptr(out), basis)
+    elif base in ("twist", "twist_inv", "twist_dag", "twist_dag_inv"):
+        lb.orc_twist(pp, _ptr(psi), _ptr(out), int("dag" in base), int("inv" in base), basis)
+    elif base == "rotate_chiral_to_ukqcd":
+        out[...] = psi
+        lb.orc_rotate_chiral_to_ukqcd(Lc, _ptr(out))
+    else:
+        raise ValueError(op)
+    return out
+
+
+def ref_apply(op: str, L, U, psi, kappa=0.16, mu=0.01, twistSign=1) -> np.ndarray:
+    """The reference's own operator (needs oracle/_ref/libqkxref.so)."""
+    psi = np.ascontiguousarray(psi, dtype=np.float64)
+    out = np.empty_like(psi)
+    rc = ref().ref_apply(REF_OPS[op], _L(L), kappa, mu, twistSign, _ptr(U), _ptr(psi), _ptr(out))
+    if rc != 0:
+        raise ValueError(op)
+    return out
+
+
+# ---------------------------------------------------------------- BLAS / CG
+def re_dot(x, y) -> float:
+    return lib().orc_re_dot(x.shape[0], _ptr(x), _ptr(y))
+
+
+def norm2(x) -> float:
+    return lib().orc_norm2(x.shape[0], _ptr(x))
+
+
+def axpy(a, y, x) -> None:
+    lib().orc_axpy(x.shape[0], a, _ptr(y), _ptr(x))
+
+
+def xpay(a, y, x) -> None:
+    lib().orc_xpay(x.shape[0], a, _ptr(y), _ptr(x))
+
+
+def cg(L, U, b, kappa, mu, twistSign=1, tol=1e-10, maxIter=1000, x0=None):
+    """CG on M^dag M (lib/solvers.cpp:16-81).  Returns (x, iterations, r2 trace)."""
+    x = np.zeros_like(b) if x0 is None else x0.copy()
+    p = params(L, kappa, mu, twistSign, -1, tol, maxIter)
+    trace = np.zeros(maxIter + 1)
+    lib().orc_cg.argtypes = [C.POINTER(OrcParams), _dp, _dp, _dp, _dp, C.c_int]
+    k = lib().orc_cg(C.byref(p), _ptr(U), _ptr(np.ascontiguousarray(b)), _ptr(x), _ptr(trace),
+                     maxIter + 1)
+    return x, k, trace[: k + 1]
+
+
+def ref_cg(L, U, b, kappa, mu, twistSign=1, tol=1e-10, maxIter=1000, x0=None):
+    x = np.zeros_like(b) if x0 is None else x0.copy()
+    ref().ref_cg(_L(L), kappa, mu, twistSign, tol, maxIter, _ptr(U),
+                 _ptr(np.ascontiguousarray(b)), _ptr(x))
+    return x
+
+
+def rel_err(a, b) -> float:
+    nb = np.linalg.norm(b.ravel())
+    return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))

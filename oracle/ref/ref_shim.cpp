@@ -1,0 +1,206 @@
+/*
+ * ref_shim.cpp -- C entry points around the reference's own classes, compiled
+ * together with the unmodified reference sources into oracle/_ref/libqkxref.so.
+ * TEST INFRASTRUCTURE ONLY: it lets the tests run the reference's Vector::tm,
+ * tm_xx, chiral variants, BLAS and CG::operator() on plain arrays so the CPU
+ * restatement (oracle/qkx_oracle.c) and the golden vectors are pinned to the
+ * reference itself.  Single rank, P = (1,1,1,1), the MPI calls go to ref/mpi.h.
+ *
+ * Arrays use the reference layouts: spinor Vector::M [V][4][3] complex,
+ * gauge Gauge::M [V][4][3][3] complex (include/lattice_util.h:90, 198).
+ */
+#include <qkxTM.h>
+#include <lattice_util.h>
+#include <blas_qkxTM.h>
+#include <solvers.h>
+
+#include <fcntl.h>
+#include <unistd.h>
+
+using namespace qkxTM;
+
+namespace {
+
+LatticeInfo make_info(const int L[4], double kappa, double mu, int twistSign, int boundaryT,
+                      double tol, int maxIter) {
+  LatticeInfo li;
+  for (int i = 0; i < 4; i++) {
+    li.L[i] = L[i];
+    li.P[i] = 1;
+  }
+  li.Nprocs = 1;
+  li.rank = 0;
+  li.kappa = kappa;
+  li.mu = mu;
+  li.twistSign = twistSign;
+  li.boundaryT = boundaryT;
+  li.tol = tol;
+  li.maxIter = maxIter;
+  return li;
+}
+
+long volume(const int L[4]) { return (long)L[0] * L[1] * L[2] * L[3]; }
+
+void load_vec(Vector& v, const double* a) {
+  memcpy(&(v.M[0][0][0]), a, sizeof(double) * 24 * v.lV4d);
+}
+void store_vec(const Vector& v, double* a) {
+  memcpy(a, &(v.M[0][0][0]), sizeof(double) * 24 * v.lV4d);
+}
+
+/* silence the reference's per-iteration prints (lib/solvers.cpp:49) */
+struct QuietStdout {
+  int saved;
+  QuietStdout() {
+    fflush(stdout);
+    saved = dup(1);
+    int devnull = open("/dev/null", O_WRONLY);
+    dup2(devnull, 1);
+    close(devnull);
+  }
+  ~QuietStdout() {
+    fflush(stdout);
+    dup2(saved, 1);
+    close(saved);
+  }
+};
+
+}  // namespace
+
+extern "C" {
+
+enum {
+  REF_DSLASH = 0,
+  REF_DSLASH_DAG = 1,
+  REF_TM = 2,
+  REF_TM_DAG = 3,
+  REF_TM_DAGTM = 4,
+  REF_WILSON = 5,
+  REF_TM_XX_EE = 6,
+  REF_TM_XX_OO = 7,
+  REF_TM_XX_DAGTM_XX_EE = 8,
+  REF_TM_XX_DAGTM_XX_OO = 9,
+  REF_DSLASH_CHIRAL = 10,
+  REF_TM_CHIRAL = 11,
+  REF_TM_XX_CHIRAL_EE = 12,
+  REF_TM_XX_CHIRAL_OO = 13,
+  REF_TM_XX_DAGTM_XX_CHIRAL_EE = 14,
+  REF_TM_XX_DAGTM_XX_CHIRAL_OO = 15,
+  REF_GAMMA5 = 16,
+  REF_GAMMA5_CHIRAL = 17,
+  REF_TWIST = 18,
+  REF_TWIST_INV = 19,
+  REF_TWIST_DAG = 20,
+  REF_TWIST_DAG_INV = 21,
+  REF_TWIST_INV_CHIRAL = 22,
+  REF_DSLASH_XX_EO = 23,
+  REF_DSLASH_XX_OE = 24,
+  REF_ROTATE_CHIRAL_TO_UKQCD = 25,
+  REF_DSLASH_XX_CHIRAL_EO = 26,
+  REF_DSLASH_XX_CHIRAL_OE = 27,
+  REF_NUM_OPS = 28
+};
+
+int ref_num_ops(void) { return REF_NUM_OPS; }
+
+/* Apply one reference operator: out = op(in).  Returns 0, or -1 for an unknown op. */
+int ref_apply(int op, const int L[4], double kappa, double mu, int twistSign, const double* U,
+              const double* in, double* out) {
+  LatticeInfo li = make_info(L, kappa, mu, twistSign, -1, 1e-10, 1000);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  Vector psi(&li), res(&li), tmp(&li);
+  load_vec(psi, in);
+  res.zero();
+  tmp.zero();
+  switch (op) {
+    case REF_DSLASH: res.applyDslash(psi, u); break;
+    case REF_DSLASH_DAG: res.applyDslashDag(psi, u); break;
+    case REF_TM: res.tm(psi, u, &li); break;
+    case REF_TM_DAG: res.tmDag(psi, u, &li); break;
+    case REF_TM_DAGTM: res.tmDagtm(psi, tmp, u, &li); break;
+    case REF_WILSON: res.Wilson(psi, u, &li); break;
+    case REF_TM_XX_EE: res.tm_xx(psi, u, &li, EE); break;
+    case REF_TM_XX_OO: res.tm_xx(psi, u, &li, OO); break;
+    case REF_TM_XX_DAGTM_XX_EE: res.tm_xxDagTm_xx(psi, u, &li, EE); break;
+    case REF_TM_XX_DAGTM_XX_OO: res.tm_xxDagTm_xx(psi, u, &li, OO); break;
+    case REF_DSLASH_CHIRAL: res.applyDslash_chiral(psi, u); break;
+    case REF_TM_CHIRAL: res.tm_chiral(psi, u, &li); break;
+    case REF_TM_XX_CHIRAL_EE: res.tm_xx_chiral(psi, u, &li, EE); break;
+    case REF_TM_XX_CHIRAL_OO: res.tm_xx_chiral(psi, u, &li, OO); break;
+    case REF_TM_XX_DAGTM_XX_CHIRAL_EE: res.tm_xxDagTm_xx_chiral(psi, u, &li, EE); break;
+    case REF_TM_XX_DAGTM_XX_CHIRAL_OO: res.tm_xxDagTm_xx_chiral(psi, u, &li, OO); break;
+    case REF_GAMMA5: res.applyGamma5(psi, &li); break;
+    case REF_GAMMA5_CHIRAL: res.applyGamma5_chiral(psi, &li); break;
+    case REF_TWIST: res.applyTwist(psi, &li); break;
+    case REF_TWIST_INV: res.applyTwistInv(psi, &li); break;
+    case REF_TWIST_DAG: res.applyTwistDag(psi, &li); break;
+    case REF_TWIST_DAG_INV: res.applyTwistDagInv(psi, &li); break;
+    case REF_TWIST_INV_CHIRAL: res.applyTwistInv_chiral(psi, &li); break;
+    case REF_DSLASH_XX_EO: res.applyDslash_xx(psi, u, EO); break;
+    case REF_DSLASH_XX_OE: res.applyDslash_xx(psi, u, OE); break;
+    case REF_ROTATE_CHIRAL_TO_UKQCD:
+      res.copy(psi);
+      res.rotateFromChiralToUKQCD();
+      break;
+    case REF_DSLASH_XX_CHIRAL_EO: res.applyDslash_xx_chiral(psi, u, EO); break;
+    case REF_DSLASH_XX_CHIRAL_OE: res.applyDslash_xx_chiral(psi, u, OE); break;
+    default: return -1;
+  }
+  store_vec(res, out);
+  return 0;
+}
+
+/* Gauge::applyBoundaryCondition on a plain array. */
+void ref_apply_bc(const int L[4], int boundaryT, double* U) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, boundaryT, 1e-10, 1000);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  {
+    QuietStdout q;
+    u.applyBoundaryCondition(&li);
+  }
+  memcpy(U, &(u.M[0][0][0][0]), sizeof(double) * 72 * volume(L));
+}
+
+/* BLAS of lib/blas_qkxTM.cpp on plain arrays.  which: 0 reCdotXdagY(x,y),
+ * 1 X_eq_X_p_aY (x updated), 2 X_eq_aX_p_Y (x updated), 3 Vector::norm2(x). */
+double ref_blas(int which, const int L[4], double a, double* x, const double* y) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Vector vx(&li), vy(&li);
+  load_vec(vx, x);
+  load_vec(vy, y);
+  double r = 0;
+  switch (which) {
+    case 0: r = reCdotXdagY(vx, vy); break;
+    case 1: X_eq_X_p_aY(vx, a, vy); break;
+    case 2: X_eq_aX_p_Y(vx, a, vy); break;
+    case 3: r = vx.norm2(); break;
+  }
+  store_vec(vx, x);
+  return r;
+}
+
+/* CG::operator()(out, in) with the links as given (the caller applies the
+ * boundary condition beforehand, as bin/test_invert.cpp:106 does).  x is both
+ * the initial content of `out` and the result.  When max_iter_run > 0 the
+ * solver runs with maxIter = max_iter_run regardless of tol (used to time a
+ * bounded number of iterations). */
+void ref_cg(const int L[4], double kappa, double mu, int twistSign, double tol, int maxIter,
+            const double* U, const double* in, double* x) {
+  LatticeInfo li = make_info(L, kappa, mu, twistSign, -1, tol, maxIter);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  u.constGauge = true;
+  Vector vin(&li), vout(&li);
+  load_vec(vin, in);
+  load_vec(vout, x);
+  {
+    QuietStdout q;
+    CG cg(&li, u);
+    cg(vout, vin, &li);
+  }
+  store_vec(vout, x);
+}
+
+}  // extern "C"

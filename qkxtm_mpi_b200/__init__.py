@@ -1,0 +1,388 @@
+"""qkxtm_mpi_b200 -- the twisted-mass Dslash / CG hot path of qkxTM_MPI on B200.
+
+This module is a thin ctypes layer over the C ABI in ``include/qkx_b200.h``
+(``libqkx_b200.so``, built in-tree by ``qkxtm_mpi_b200.build``).  It mirrors the
+reference's hot-path interface by name:
+
+* ``LatticeInfo``            -- struct LatticeInfo (include/qkxTM.h:156-204)
+* ``Lattice.tm / tmDag / tmDagtm / Wilson / tm_xx / tm_xxDagTm_xx / *_chiral``
+                             -- qkxTM::Vector members (lib/lattice_util.cpp:1148-2071)
+* ``Lattice.cg``             -- CG::operator() (lib/solvers.cpp:16-81)
+* ``Lattice.reCdotXdagY / X_eq_X_p_aY / X_eq_aX_p_Y / norm2``
+                             -- lib/blas_qkxTM.cpp, Vector::norm2
+* ``Lattice.invert``         -- the solve sequence tmDag + CG of bin/test_invert.cpp,
+                                with the B200 solvers (plain FP64 or even-odd mixed precision)
+
+Fields are numpy float64 arrays in the reference's host layouts: spinor
+``[V, 4, 3, 2]`` (Vector::M) and gauge ``[V, 4, 3, 3, 2]`` (Gauge::M).
+
+There is no CPU fallback: importing works without a GPU, but every call that
+computes goes through the CUDA library and raises ``QkxError`` if it is
+missing or fails.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, field
+from typing import Sequence
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libqkx_b200.so")
+
+OK = 0
+ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOGAUGE, ERR_NOT_CONVERGED, ERR_NAN, ERR_UNSUPPORTED = (
+    -1, -2, -3, -4, -5, -6, -7)
+
+LINKS_AS_GIVEN, LINKS_APPLY_BC = 0, 1
+SOLVER_CG_FP64, SOLVER_CG_EO_MIXED = 0, 1
+PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
+
+# operator ids of enum qkx_op
+OPS = {
+    "dslash": 0, "dslash_dag": 1, "tm": 2, "tm_dag": 3, "tm_dagtm": 4, "wilson": 5,
+    "tm_xx_ee": 6, "tm_xx_oo": 7, "tm_xx_dagtm_xx_ee": 8, "tm_xx_dagtm_xx_oo": 9,
+    "dslash_chiral": 10, "tm_chiral": 11, "tm_xx_chiral_ee": 12, "tm_xx_chiral_oo": 13,
+    "tm_xx_dagtm_xx_chiral_ee": 14, "tm_xx_dagtm_xx_chiral_oo": 15, "gamma5": 16,
+    "gamma5_chiral": 17, "twist": 18, "twist_inv": 19, "twist_dag": 20, "twist_dag_inv": 21,
+    "twist_inv_chiral": 22, "dslash_xx_eo": 23, "dslash_xx_oe": 24,
+    "rotate_chiral_to_ukqcd": 25, "dslash_xx_chiral_eo": 26, "dslash_xx_chiral_oe": 27,
+    "tm_dag_chiral": 28, "tm_dagtm_chiral": 29,
+}
+
+# exported symbols of include/qkx_b200.h (checked by the CPU tests)
+SYMBOLS = [
+    "qkx_version", "qkx_last_error", "qkx_create", "qkx_destroy", "qkx_set_params",
+    "qkx_get_params", "qkx_sync", "qkx_stream", "qkx_spinor_bytes", "qkx_volume",
+    "qkx_load_gauge", "qkx_gauge_generate", "qkx_download_gauge", "qkx_gauge_compressible",
+    "qkx_apply", "qkx_apply_dev", "qkx_spinor_upload", "qkx_spinor_download",
+    "qkx_reCdotXdagY", "qkx_X_eq_X_p_aY", "qkx_X_eq_aX_p_Y", "qkx_norm2",
+    "qkx_cg", "qkx_cg_dev", "qkx_invert", "qkx_invert_dev",
+    "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
+    "qkx_memcpy_h2d", "qkx_memcpy_d2h",
+    "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset",
+]
+
+
+class QkxError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"qkx error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    _fields_ = [("L", C.c_int * 4), ("kappa", C.c_double), ("mu", C.c_double),
+                ("twistSign", C.c_int), ("boundaryT", C.c_int), ("tol", C.c_double),
+                ("maxIter", C.c_int), ("reliableDelta", C.c_double)]
+
+
+class SolverParams(C.Structure):
+    _fields_ = [("method", C.c_int), ("sloppy_precision", C.c_int), ("tol", C.c_double),
+                ("maxIter", C.c_int), ("reliable_delta", C.c_double), ("use_graphs", C.c_int)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("reliable_updates", C.c_int), ("converged", C.c_int),
+                ("restarts", C.c_int), ("true_residual", C.c_double),
+                ("normal_residual", C.c_double), ("seconds", C.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+_lib = None
+_vp, _dp = C.c_void_p, C.POINTER(C.c_double)
+
+
+def lib() -> C.CDLL:
+    """Load libqkx_b200.so (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise QkxError(ERR_UNSUPPORTED,
+                           f"{LIB_PATH} is missing: run `python -m qkxtm_mpi_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        L.qkx_version.restype = C.c_char_p
+        L.qkx_last_error.restype = C.c_char_p
+        L.qkx_create.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(_vp)]
+        L.qkx_destroy.argtypes = [_vp]
+        L.qkx_destroy.restype = None
+        L.qkx_set_params.argtypes = [_vp, C.POINTER(Params)]
+        L.qkx_get_params.argtypes = [_vp, C.POINTER(Params)]
+        L.qkx_sync.argtypes = [_vp]
+        L.qkx_stream.argtypes = [_vp]
+        L.qkx_stream.restype = _vp
+        L.qkx_spinor_bytes.argtypes = [_vp]
+        L.qkx_spinor_bytes.restype = C.c_size_t
+        L.qkx_volume.argtypes = [_vp]
+        L.qkx_volume.restype = C.c_size_t
+        L.qkx_load_gauge.argtypes = [_vp, _vp, C.c_int]
+        L.qkx_gauge_generate.argtypes = [_vp, C.c_double, C.c_ulonglong, C.c_int]
+        L.qkx_download_gauge.argtypes = [_vp, _vp]
+        L.qkx_gauge_compressible.argtypes = [_vp]
+        L.qkx_apply.argtypes = [_vp, C.c_int, _vp, _vp]
+        L.qkx_apply_dev.argtypes = [_vp, C.c_int, _vp, _vp]
+        L.qkx_spinor_upload.argtypes = [_vp, _vp, _vp]
+        L.qkx_spinor_download.argtypes = [_vp, _vp, _vp]
+        L.qkx_reCdotXdagY.argtypes = [_vp, _vp, _vp, _dp]
+        L.qkx_norm2.argtypes = [_vp, _vp, _dp]
+        L.qkx_X_eq_X_p_aY.argtypes = [_vp, _vp, C.c_double, _vp]
+        L.qkx_X_eq_aX_p_Y.argtypes = [_vp, _vp, C.c_double, _vp]
+        L.qkx_cg.argtypes = [_vp, _vp, _vp, C.POINTER(SolveInfo)]
+        L.qkx_cg_dev.argtypes = [_vp, _vp, _vp, C.POINTER(SolveInfo)]
+        L.qkx_invert.argtypes = [_vp, C.POINTER(SolverParams), C.c_int, C.POINTER(_vp),
+                                 C.POINTER(_vp), C.POINTER(SolveInfo)]
+        L.qkx_invert_dev.argtypes = L.qkx_invert.argtypes
+        L.qkx_host_alloc.argtypes = [C.c_size_t]
+        L.qkx_host_alloc.restype = _vp
+        L.qkx_host_free.argtypes = [_vp]
+        L.qkx_host_free.restype = None
+        L.qkx_device_alloc.argtypes = [_vp, C.c_size_t]
+        L.qkx_device_alloc.restype = _vp
+        L.qkx_device_free.argtypes = [_vp, _vp]
+        L.qkx_device_free.restype = None
+        L.qkx_memcpy_h2d.argtypes = [_vp, _vp, _vp, C.c_size_t]
+        L.qkx_memcpy_d2h.argtypes = [_vp, _vp, _vp, C.c_size_t]
+        L.qkx_profile_enable.argtypes = [_vp, C.c_int]
+        L.qkx_profile_read.argtypes = [_vp, C.POINTER(C.c_longlong), _dp, _dp]
+        L.qkx_profile_reset.argtypes = [_vp]
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc != OK:
+        raise QkxError(rc, lib().qkx_last_error().decode())
+    return rc
+
+
+def version() -> str:
+    return lib().qkx_version().decode()
+
+
+@dataclass
+class LatticeInfo:
+    """The hot-path fields of the reference's struct LatticeInfo (include/qkxTM.h:156-204),
+    with the reference's defaults."""
+    L: Sequence[int] = (8, 8, 8, 16)
+    kappa: float = 0.16
+    mu: float = 0.008
+    twistSign: int = 1
+    boundaryT: int = -1
+    tol: float = 1e-1
+    maxIter: int = 1000
+    reliableDelta: float = 0.1
+
+    def to_c(self) -> Params:
+        return Params((C.c_int * 4)(*self.L), self.kappa, self.mu, self.twistSign, self.boundaryT,
+                      self.tol, int(self.maxIter), self.reliableDelta)
+
+
+def _host(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    return a
+
+
+class DeviceField:
+    """A device spinor in the library's even-odd layout (owned, freed on close)."""
+
+    def __init__(self, lat: "Lattice"):
+        self.lat = lat
+        self.nbytes = lib().qkx_spinor_bytes(lat.ctx)
+        self.ptr = lib().qkx_device_alloc(lat.ctx, self.nbytes)
+        if not self.ptr:
+            raise QkxError(ERR_NOMEM, "device allocation failed")
+
+    def upload(self, host: np.ndarray) -> "DeviceField":
+        h = _host(host)
+        check(lib().qkx_spinor_upload(self.lat.ctx, h.ctypes.data, self.ptr))
+        check(lib().qkx_sync(self.lat.ctx))
+        return self
+
+    def download(self) -> np.ndarray:
+        out = np.empty((self.lat.V, 4, 3, 2))
+        check(lib().qkx_spinor_download(self.lat.ctx, self.ptr, out.ctypes.data))
+        return out
+
+    def close(self):
+        if self.ptr:
+            lib().qkx_device_free(self.lat.ctx, self.ptr)
+            self.ptr = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Lattice:
+    """One lattice on one GPU: gauge field, operators, BLAS and solvers."""
+
+    def __init__(self, info: LatticeInfo, device: int = 0):
+        self.info = info
+        self.L = tuple(int(v) for v in info.L)
+        self.V = int(np.prod(self.L))
+        ctx = _vp()
+        p = info.to_c()
+        check(lib().qkx_create(C.byref(p), device, C.byref(ctx)))
+        self.ctx = ctx
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().qkx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_params(self, **kw) -> None:
+        for k, v in kw.items():
+            setattr(self.info, k, v)
+        p = self.info.to_c()
+        check(lib().qkx_set_params(self.ctx, C.byref(p)))
+
+    # ------------------------------------------------------------ gauge
+    def load_gauge(self, U: np.ndarray, bc_mode: int = LINKS_AS_GIVEN) -> None:
+        U = _host(U)
+        assert U.size == self.V * 72, "gauge must be [V,4,3,3,2] float64"
+        check(lib().qkx_load_gauge(self.ctx, U.ctypes.data, bc_mode))
+
+    def generate_gauge(self, eps: float, seed: int, bc_mode: int = LINKS_APPLY_BC) -> None:
+        check(lib().qkx_gauge_generate(self.ctx, eps, seed, bc_mode))
+
+    def download_gauge(self) -> np.ndarray:
+        U = np.empty((self.V, 4, 3, 3, 2))
+        check(lib().qkx_download_gauge(self.ctx, U.ctypes.data))
+        return U
+
+    def compressible(self) -> bool:
+        return check_nonneg(lib().qkx_gauge_compressible(self.ctx)) == 1
+
+    # ------------------------------------------------------------ operators
+    def apply(self, op: str, psi: np.ndarray) -> np.ndarray:
+        psi = _host(psi)
+        assert psi.size == self.V * 24, "spinor must be [V,4,3,2] float64"
+        out = np.empty((self.V, 4, 3, 2))
+        check(lib().qkx_apply(self.ctx, OPS[op], psi.ctypes.data, out.ctypes.data))
+        return out
+
+    def apply_dev(self, op: str, src: DeviceField, dst: DeviceField) -> None:
+        check(lib().qkx_apply_dev(self.ctx, OPS[op], src.ptr, dst.ptr))
+
+    # reference names (lib/lattice_util.cpp)
+    def applyDslash(self, psi): return self.apply("dslash", psi)
+    def applyDslashDag(self, psi): return self.apply("dslash_dag", psi)
+    def tm(self, psi): return self.apply("tm", psi)
+    def tmDag(self, psi): return self.apply("tm_dag", psi)
+    def tmDagtm(self, psi): return self.apply("tm_dagtm", psi)
+    def Wilson(self, psi): return self.apply("wilson", psi)
+    def applyGamma5(self, psi): return self.apply("gamma5", psi)
+
+    def tm_xx(self, psi, parity: str = "EE"):
+        return self.apply("tm_xx_" + parity.lower(), psi)
+
+    def tm_xxDagTm_xx(self, psi, parity: str = "EE"):
+        return self.apply("tm_xx_dagtm_xx_" + parity.lower(), psi)
+
+    def tm_chiral(self, psi): return self.apply("tm_chiral", psi)
+
+    def tm_xx_chiral(self, psi, parity: str = "EE"):
+        return self.apply("tm_xx_chiral_" + parity.lower(), psi)
+
+    def tm_xxDagTm_xx_chiral(self, psi, parity: str = "EE"):
+        return self.apply("tm_xx_dagtm_xx_chiral_" + parity.lower(), psi)
+
+    def field(self, host: np.ndarray | None = None) -> DeviceField:
+        f = DeviceField(self)
+        if host is not None:
+            f.upload(host)
+        return f
+
+    # ------------------------------------------------------------ BLAS (device fields)
+    def reCdotXdagY(self, x: DeviceField, y: DeviceField) -> float:
+        r = C.c_double()
+        check(lib().qkx_reCdotXdagY(self.ctx, x.ptr, y.ptr, C.byref(r)))
+        return r.value
+
+    def norm2(self, x: DeviceField) -> float:
+        r = C.c_double()
+        check(lib().qkx_norm2(self.ctx, x.ptr, C.byref(r)))
+        return r.value
+
+    def X_eq_X_p_aY(self, x: DeviceField, a: float, y: DeviceField) -> None:
+        check(lib().qkx_X_eq_X_p_aY(self.ctx, x.ptr, a, y.ptr))
+
+    def X_eq_aX_p_Y(self, x: DeviceField, a: float, y: DeviceField) -> None:
+        check(lib().qkx_X_eq_aX_p_Y(self.ctx, x.ptr, a, y.ptr))
+
+    # ------------------------------------------------------------ solvers
+    def cg(self, in_: np.ndarray, x: np.ndarray | None = None):
+        """CG::operator()(x, in): x += (M^+M)^-1 in, reference stopping rule."""
+        in_ = _host(in_)
+        x = np.zeros((self.V, 4, 3, 2)) if x is None else _host(x).copy()
+        info = SolveInfo()
+        rc = lib().qkx_cg(self.ctx, in_.ctypes.data, x.ctypes.data, C.byref(info))
+        if rc not in (OK, ERR_NOT_CONVERGED):
+            check(rc)
+        return x, info
+
+    def invert(self, bs: Sequence[np.ndarray], method: int = SOLVER_CG_EO_MIXED,
+               precision: int = PREC_HALF, tol: float = 1e-10, maxIter: int = 10000,
+               reliable_delta: float = 0.1, use_graphs: int = 1, strict: bool = True):
+        """Solve M x_i = b_i to ||b - M x|| / ||b|| <= tol (FP64 true residual)."""
+        bs = [_host(b) for b in bs]
+        xs = [np.empty((self.V, 4, 3, 2)) for _ in bs]
+        n = len(bs)
+        bp = (_vp * n)(*[b.ctypes.data for b in bs])
+        xp = (_vp * n)(*[x.ctypes.data for x in xs])
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        info = SolveInfo()
+        rc = lib().qkx_invert(self.ctx, C.byref(sp), n, bp, xp, C.byref(info))
+        if rc != OK and (strict or rc != ERR_NOT_CONVERGED):
+            check(rc)
+        return xs, info
+
+    def invert_dev(self, bs: Sequence[DeviceField], xs: Sequence[DeviceField],
+                   method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF,
+                   tol: float = 1e-10, maxIter: int = 10000, reliable_delta: float = 0.1,
+                   use_graphs: int = 1) -> SolveInfo:
+        n = len(bs)
+        bp = (_vp * n)(*[b.ptr for b in bs])
+        xp = (_vp * n)(*[x.ptr for x in xs])
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        info = SolveInfo()
+        check(lib().qkx_invert_dev(self.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
+        return info
+
+    # ------------------------------------------------------------ profiling
+    def profile(self, on: bool) -> None:
+        check(lib().qkx_profile_enable(self.ctx, int(on)))
+
+    def profile_read(self):
+        n, ms, by = C.c_longlong(), C.c_double(), C.c_double()
+        check(lib().qkx_profile_read(self.ctx, C.byref(n), C.byref(ms), C.byref(by)))
+        return n.value, ms.value, by.value
+
+    def profile_reset(self) -> None:
+        check(lib().qkx_profile_reset(self.ctx))
+
+    def sync(self) -> None:
+        check(lib().qkx_sync(self.ctx))
+
+
+def check_nonneg(rc: int) -> int:
+    if rc < 0:
+        check(rc)
+    return rc

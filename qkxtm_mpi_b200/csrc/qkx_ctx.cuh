@@ -1,0 +1,101 @@
+// qkx_ctx.cuh -- the context behind the C ABI (internal to libqkx_b200.so).
+#pragma once
+#include <stdarg.h>
+#include <stdio.h>
+
+#include <string>
+#include <vector>
+
+#include "qkx_b200.h"
+#include "blas.cuh"
+#include "qkx_common.cuh"
+
+namespace qkx {
+void set_error(const char* fmt, ...);
+struct MixedState;
+}  // namespace qkx
+
+#define QKX_CUDA(call)                                                                                \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess) {                                                                          \
+      qkx::set_error("%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__);     \
+      return QKX_ERR_CUDA;                                                                            \
+    }                                                                                                 \
+  } while (0)
+
+#define QKX_TRY(expr)        \
+  do {                       \
+    int rc_ = (expr);        \
+    if (rc_ != QKX_OK) return rc_; \
+  } while (0)
+
+struct qkx_ctx {
+  qkx_params p;
+  int device = 0;
+  cudaStream_t st = nullptr;
+  int Vh = 0;
+  size_t V = 0;
+  qkx::Geom geom{};      // links exactly as the operator uses them (bc_sign +1)
+  qkx::Geom geom_raw{};  // compressed SU(3) links, boundary sign applied in the kernels
+  int have_gauge = 0;
+  int compressible = 0;
+  int raw_sign = 1;
+  double link_unitarity = 0;  // max |U U^+ - 1|
+  double2* U18 = nullptr;     // [2][4][9][Vh] FP64, as the operator uses them
+  float4* U12f = nullptr;     // [2][4][3][Vh] FP32 12-real, SU(3)
+  uint4* U12ha = nullptr;     // [2][4][Vh]  FP16 12-real complex 0..3
+  uint2* U12hb = nullptr;     // [2][4][Vh]  FP16 12-real complex 4..5
+  double2* stage = nullptr;   // one host-layout spinor (V*12 double2)
+  static constexpr int NW = 8;
+  double2* w[NW] = {};        // FP64 full-lattice work fields
+  double* part = nullptr;     // reduction partials
+  int npart = 0;
+  qkx::CgScalars* sc = nullptr;    // device solver scalars
+  qkx::CgScalars* sc_h = nullptr;  // pinned host mirror
+  double* dscal = nullptr;         // device scratch scalars [64]
+  double* hscal = nullptr;         // pinned host scalars [64]
+  cudaEvent_t t0 = nullptr, t1 = nullptr;
+  // profiling of the hopping kernels
+  int prof = 0;
+  std::vector<cudaEvent_t> ev_a, ev_b;
+  std::vector<double> ev_bytes;
+  size_t ev_used = 0;
+  long long prof_launches = 0;
+  double prof_ms = 0, prof_bytes = 0;
+  qkx::MixedState* mixed = nullptr;
+};
+
+namespace qkx {
+
+inline SpinorF64 F64(const double2* base, int Vh) {
+  double2* b = const_cast<double2*>(base);
+  return SpinorF64{b, b ? b + (size_t)12 * Vh : nullptr, Vh};
+}
+
+// profiling brackets around one hopping-kernel launch
+int prof_begin(qkx_ctx* c);
+int prof_end(qkx_ctx* c, double bytes);
+int prof_collect(qkx_ctx* c);
+
+// grid for the grid-stride BLAS kernels
+inline int blas_grid(size_t n) {
+  size_t b = (n + BLAS_NT - 1) / BLAS_NT;
+  return (int)(b < 148 * 8 ? (b ? b : 1) : 148 * 8);
+}
+
+// Re<x,y> over n double2, finalized into the solver scalars / dst (see FIN_*)
+int redot(qkx_ctx* c, const double2* x, const double2* y, size_t n, int mode, double* dst, int rhs);
+int finalize(qkx_ctx* c, int nparts, int mode, double* dst, int rhs);
+
+// FP64 operator on full even-odd fields (out != in)
+int run_op(qkx_ctx* c, int op, const double2* in, double2* out);
+// M (tm) or M^+ on full FP64 fields with the 18-real links, fused twist
+int apply_tm(qkx_ctx* c, const double2* in, double2* out, bool dagger);
+
+// mixed-precision solver entry (mixed.cu)
+int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
+                    double2* const* x, qkx_solve_info* info);
+void mixed_free(qkx_ctx* c);
+
+}  // namespace qkx

@@ -1,0 +1,129 @@
+"""Generate the golden vectors in tests/golden/ from the REFERENCE itself.
+
+The reference's hot-path sources are compiled unmodified (oracle/ref/Makefile)
+into oracle/_ref/libqkxref.so; this script runs the reference's own
+Vector::tm / tm_xx / chiral / BLAS / CG::operator() on seeded synthetic inputs
+and stores the outputs.  The inputs are NOT stored: they are regenerated by
+the oracle's counter-based generator from the seeds recorded here, and a
+checksum of the inputs is stored so that a change of the generator is caught.
+
+    python tests/golden/make_golden.py          (needs the reference sources)
+
+Fixtures:
+  ref_ops_small.npz   full outputs of every operator, lattice 4x2x2x4
+  ref_ops_probe.npz   per operator: |out|^2 and <w_k, out> for 3 fixed probe
+                      fields w_k, plus the full output on 16 sampled sites,
+                      lattice 4x4x4x8
+  ref_cg.npz          CG::operator() solution probes and true residual,
+                      lattices 4x4x4x8 and 8x8x8x16
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+
+KAPPA, MU = 0.16, 0.01
+EPS = 0.3
+# operators also stored with twistSign = -1
+TWIST_SIGN_OPS = ["tm", "tm_dag", "twist_inv", "tm_xx_ee", "tm_xx_dagtm_xx_oo", "tm_xx_chiral_oo",
+                  "tm_xx_dagtm_xx_chiral_ee"]
+
+
+def inputs(L, seed_u, seed_psi, bc=True):
+    U = O.gauge_random(L, EPS, seed_u)
+    if bc:
+        U = O.apply_bc(L, U, -1)
+    psi = O.spinor_gaussian(L, seed_psi)
+    return U, psi
+
+
+def checksum(a: np.ndarray) -> np.ndarray:
+    w = np.linspace(0.5, 1.5, a.size).reshape(a.shape)
+    return np.array([a.sum(), (a * w).sum(), (a * a).sum()])
+
+
+def probes(L, n=3, seed=9000):
+    return [O.spinor_gaussian(L, seed + k) for k in range(n)]
+
+
+def sample_sites(L, n=16):
+    V = O.volume(L)
+    return np.unique(np.linspace(0, V - 1, n).astype(np.int64))
+
+
+def main():
+    O.build(ref=True)
+    if not O.ref_available():
+        raise SystemExit("reference build missing (oracle/_ref/libqkxref.so)")
+
+    # --- small lattice, full outputs
+    L = (4, 2, 2, 4)
+    U, psi = inputs(L, 11, 12)
+    d = {"L": np.array(L), "kappa": KAPPA, "mu": MU, "eps": EPS, "seed_u": 11, "seed_psi": 12,
+         "bc": 1, "in_checksum": np.concatenate([checksum(U), checksum(psi)])}
+    for op in O.REF_OPS:
+        d[f"{op}@1"] = O.ref_apply(op, L, U, psi, KAPPA, MU, 1)
+    for op in TWIST_SIGN_OPS:
+        d[f"{op}@-1"] = O.ref_apply(op, L, U, psi, KAPPA, MU, -1)
+    np.savez_compressed(os.path.join(HERE, "ref_ops_small.npz"), **d)
+
+    # --- 4^3x8, probes
+    L = (4, 4, 4, 8)
+    U, psi = inputs(L, 21, 22)
+    W = probes(L)
+    sites = sample_sites(L)
+    d = {"L": np.array(L), "kappa": KAPPA, "mu": MU, "eps": EPS, "seed_u": 21, "seed_psi": 22,
+         "bc": 1, "probe_seed": 9000, "sites": sites,
+         "in_checksum": np.concatenate([checksum(U), checksum(psi)])}
+    for op in O.REF_OPS:
+        out = O.ref_apply(op, L, U, psi, KAPPA, MU, 1)
+        d[f"{op}:norm2"] = np.array([np.sum(out * out)])
+        d[f"{op}:probe"] = np.array([np.sum(w * out) for w in W])
+        d[f"{op}:sites"] = out[sites]
+    # BLAS of the reference
+    x = psi.copy()
+    y = O.spinor_gaussian(L, 23)
+    d["blas:redot"] = np.array([O.ref().ref_blas(0, O._L(L), 0.0, O._ptr(x.copy()), O._ptr(y))])
+    x1 = x.copy()
+    O.ref().ref_blas(1, O._L(L), 0.37, O._ptr(x1), O._ptr(y))
+    d["blas:axpy:sites"] = x1[sites]
+    x2 = x.copy()
+    O.ref().ref_blas(2, O._L(L), -0.41, O._ptr(x2), O._ptr(y))
+    d["blas:xpay:sites"] = x2[sites]
+    d["blas:norm2"] = np.array([O.ref().ref_blas(3, O._L(L), 0.0, O._ptr(x.copy()), O._ptr(y))])
+    np.savez_compressed(os.path.join(HERE, "ref_ops_probe.npz"), **d)
+
+    # --- CG::operator() (lib/solvers.cpp) as bin/test_invert.cpp drives it:
+    # in = M^+ b, links with the antiperiodic boundary applied, x zero.
+    d = {}
+    for tag, L, seed_u, seed_b in (("4x4x4x8", (4, 4, 4, 8), 31, 32), ("8x8x8x16", (8, 8, 8, 16), 41, 42)):
+        U, b = inputs(L, seed_u, seed_b)
+        Mdb = O.ref_apply("tm_dag", L, U, b, KAPPA, MU, 1)
+        xr = O.ref_cg(L, U, Mdb, KAPPA, MU, 1, tol=1e-10, maxIter=1000)
+        W = probes(L)
+        res = b - O.ref_apply("tm", L, U, xr, KAPPA, MU, 1)
+        d[f"{tag}:L"] = np.array(L)
+        d[f"{tag}:seeds"] = np.array([seed_u, seed_b])
+        d[f"{tag}:x_norm2"] = np.array([np.sum(xr * xr)])
+        d[f"{tag}:x_probe"] = np.array([np.sum(w * xr) for w in W])
+        d[f"{tag}:x_sites"] = xr[sample_sites(L)]
+        d[f"{tag}:true_residual"] = np.array([np.sqrt(np.sum(res * res) / np.sum(b * b))])
+        _, iters, trace = O.cg(L, U, Mdb, KAPPA, MU, 1, tol=1e-10, maxIter=1000)
+        d[f"{tag}:iters_oracle"] = np.array([iters])
+        d[f"{tag}:r2_trace_oracle"] = trace
+        d[f"{tag}:in_checksum"] = np.concatenate([checksum(U), checksum(b)])
+    d["kappa"], d["mu"], d["eps"] = KAPPA, MU, EPS
+    np.savez_compressed(os.path.join(HERE, "ref_cg.npz"), **d)
+    for f in ("ref_ops_small.npz", "ref_ops_probe.npz", "ref_cg.npz"):
+        print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,90 @@
+"""CPU tests of the C-ABI boundary: the library builds, loads, and exports every
+entry point declared in include/*.h; argument checking happens before any
+CUDA call.  No compute is run here."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+from conftest import ROOT, gpu_available
+
+
+def _header_functions():
+    names = set()
+    for h in os.listdir(os.path.join(ROOT, "include")):
+        if not h.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", h)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"\b(qkx_\w+)\s*\(", text):
+            names.add(m.group(1))
+    return names
+
+
+@pytest.fixture(scope="module")
+def built_lib():
+    from qkxtm_mpi_b200 import build
+    if not os.path.exists(build.LIB):
+        build.build()
+    return build.LIB
+
+
+def test_header_declares_the_package_symbols():
+    import qkxtm_mpi_b200 as Q
+    assert _header_functions() == set(Q.SYMBOLS)
+
+
+def test_library_exports_every_declared_symbol(built_lib):
+    out = subprocess.run(["nm", "-D", "--defined-only", built_lib], capture_output=True, text=True,
+                         check=True).stdout
+    exported = {line.split()[-1] for line in out.splitlines() if line.strip()}
+    missing = _header_functions() - exported
+    assert not missing, missing
+    # nothing else leaks out of the library under a qkx_ prefix
+    extra = {s for s in exported if s.startswith("qkx_")} - _header_functions()
+    assert not extra, extra
+
+
+def test_library_loads_and_reports_version(built_lib):
+    import qkxtm_mpi_b200 as Q
+    assert "sm_100a" in Q.version()
+    assert Q.lib().qkx_last_error() is not None
+
+
+def test_parameter_checks_need_no_device(built_lib):
+    import qkxtm_mpi_b200 as Q
+    L = Q.lib()
+    ctx = C.c_void_p()
+    bad = [
+        Q.LatticeInfo(L=(3, 4, 4, 4)),           # odd L[0]: the even-odd layout needs it even
+        Q.LatticeInfo(L=(4, 4, 4, 1)),           # extent below 2
+        Q.LatticeInfo(L=(4, 4, 4, 4), twistSign=2),
+        Q.LatticeInfo(L=(4, 4, 4, 4), boundaryT=0),
+    ]
+    for info in bad:
+        p = info.to_c()
+        rc = L.qkx_create(C.byref(p), 0, C.byref(ctx))
+        assert rc == Q.ERR_INVALID
+        assert L.qkx_last_error().decode().startswith("invalid argument")
+        assert not ctx.value
+    assert L.qkx_create(None, 0, C.byref(ctx)) == Q.ERR_INVALID
+
+
+def test_null_context_is_rejected(built_lib):
+    import qkxtm_mpi_b200 as Q
+    L = Q.lib()
+    assert L.qkx_apply(None, 0, None, None) == Q.ERR_INVALID
+    assert L.qkx_load_gauge(None, None, 0) == Q.ERR_INVALID
+    assert L.qkx_spinor_bytes(None) == 0
+    L.qkx_destroy(None)
+
+
+def test_create_without_gpu_fails_cleanly(built_lib):
+    if gpu_available():
+        pytest.skip("a GPU is present")
+    import qkxtm_mpi_b200 as Q
+    with pytest.raises(Q.QkxError) as e:
+        Q.Lattice(Q.LatticeInfo(L=(4, 4, 4, 4)))
+    assert e.value.code == Q.ERR_CUDA
