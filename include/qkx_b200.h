@@ -203,8 +203,11 @@ typedef struct qkx_solver_params {
   int sloppy_precision;    /* QKX_PREC_* for the inner iterations (CG_EO_MIXED) */
   double tol;              /* target for the true residual ||b - M x|| / ||b|| */
   int maxIter;             /* total iteration cap */
-  double reliable_delta;   /* FP64 residual recomputation when |r| < delta * max|r| */
-  int use_graphs;          /* capture the inner iterations in CUDA graphs */
+  double reliable_delta;   /* FP64 residual recomputation when |r| drops by this factor;
+                              <= 0 picks the default of the sloppy precision (0.1 half, 1e-3 single) */
+  int use_graphs;          /* replay the inner iteration from a CUDA graph */
+  const double* mu;        /* NULL, or nrhs twisted masses (one per right-hand side, the
+                              multi-mass solve of CG_EO_MIXED); NULL = the context's mu */
 } qkx_solver_params;
 
 /* Solve M x_i = b_i for nrhs right-hand sides (host buffers, Vector::M layout),

@@ -80,7 +80,8 @@ class Params(C.Structure):
 
 class SolverParams(C.Structure):
     _fields_ = [("method", C.c_int), ("sloppy_precision", C.c_int), ("tol", C.c_double),
-                ("maxIter", C.c_int), ("reliable_delta", C.c_double), ("use_graphs", C.c_int)]
+                ("maxIter", C.c_int), ("reliable_delta", C.c_double), ("use_graphs", C.c_int),
+                ("mu", C.POINTER(C.c_double))]
 
 
 class SolveInfo(C.Structure):
@@ -340,7 +341,7 @@ class Lattice:
 
     def invert(self, bs: Sequence[np.ndarray], method: int = SOLVER_CG_EO_MIXED,
                precision: int = PREC_HALF, tol: float = 1e-10, maxIter: int = 10000,
-               reliable_delta: float = 0.1, use_graphs: int = 1, strict: bool = True):
+               reliable_delta: float = 0.0, use_graphs: int = 1, strict: bool = True):
         """Solve M x_i = b_i to ||b - M x|| / ||b|| <= tol (FP64 true residual)."""
         bs = [_host(b) for b in bs]
         xs = [np.empty((self.V, 4, 3, 2)) for _ in bs]
@@ -356,7 +357,7 @@ class Lattice:
 
     def invert_dev(self, bs: Sequence[DeviceField], xs: Sequence[DeviceField],
                    method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF,
-                   tol: float = 1e-10, maxIter: int = 10000, reliable_delta: float = 0.1,
+                   tol: float = 1e-10, maxIter: int = 10000, reliable_delta: float = 0.0,
                    use_graphs: int = 1) -> SolveInfo:
         n = len(bs)
         bp = (_vp * n)(*[b.ptr for b in bs])

@@ -94,12 +94,12 @@ static double hop_bytes(size_t nout, double S, double G, bool both, bool extra_x
 }
 
 template <int B, bool DAG, int EPI>
-static int hop64_t(qkx_ctx* c, const double2* in, double2* out, const double2* x, int out_parity, double a,
-                   double cc, double s, double* norm_part) {
+static int hop64_t(qkx_ctx* c, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_distinct, int out_parity,
+                   double a, double cc, double s, double* norm_part) {
   HopArgs<SpinorF64, GaugeF64x18> A;
-  A.out = F64(out, c->Vh);
-  A.in = F64(in, c->Vh);
-  A.x = F64(x ? x : in, c->Vh);
+  A.out = out;
+  A.in = in;
+  A.x = x;
   A.gauge = GaugeF64x18{c->U18, c->Vh};
   A.g = c->geom;
   A.out_parity = out_parity;
@@ -107,22 +107,28 @@ static int hop64_t(qkx_ctx* c, const double2* in, double2* out, const double2* x
   A.c = cc;
   A.s = s;
   A.norm_part = norm_part;
+  A.nrhs = 1;
+  A.nblk = hop_blocks_per_rhs<128>(c->Vh, out_parity);
+  A.cvec = nullptr;
+  A.svec = nullptr;
+  A.active = nullptr;
   const int n = out_parity < 0 ? 2 * c->Vh : c->Vh;
-  const int nb = (n + 127) / 128;
   QKX_TRY(prof_begin(c));
-  hop_kernel<128, SpinorF64, GaugeF64x18, double, B, DAG, EPI><<<nb, 128, 0, c->st>>>(A);
+  hop_kernel<128, SpinorF64, GaugeF64x18, double, B, DAG, EPI><<<A.nblk, 128, 0, c->st>>>(A);
   QKX_CUDA(cudaGetLastError());
-  bool extra = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5) && x && x != in;
+  bool extra = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV) && x_distinct;
   return prof_end(c, hop_bytes(n, 192.0, 144.0, out_parity < 0, extra));
 }
 
-// runtime -> compile-time dispatch
-static int hop64(qkx_ctx* c, int basis, bool dag, int epi, const double2* in, double2* out, const double2* x,
-                 int out_parity, double a, double cc, double s, double* norm_part = nullptr) {
+// runtime -> compile-time dispatch, on accessors (single-parity fields allowed)
+int hop64a(qkx_ctx* c, int basis, bool dag, int epi, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_distinct,
+           int out_parity, double a, double cc, double s, double* norm_part) {
 #define QKX_HOP_CASE(B_, D_, E_) \
-  if (basis == B_ && dag == D_ && epi == E_) return hop64_t<B_, D_, E_>(c, in, out, x, out_parity, a, cc, s, norm_part);
+  if (basis == B_ && dag == D_ && epi == E_)   \
+    return hop64_t<B_, D_, E_>(c, in, out, x, x_distinct, out_parity, a, cc, s, norm_part);
 #define QKX_HOP_EPIS(B_, D_) \
-  QKX_HOP_CASE(B_, D_, EPI_PLAIN) QKX_HOP_CASE(B_, D_, EPI_XPAY) QKX_HOP_CASE(B_, D_, EPI_XPAY_G5) QKX_HOP_CASE(B_, D_, EPI_TWIST_INV)
+  QKX_HOP_CASE(B_, D_, EPI_PLAIN) QKX_HOP_CASE(B_, D_, EPI_XPAY) QKX_HOP_CASE(B_, D_, EPI_XPAY_G5) \
+  QKX_HOP_CASE(B_, D_, EPI_TWIST_INV) QKX_HOP_CASE(B_, D_, EPI_XPAY_TWINV)
   QKX_HOP_EPIS(0, false)
   QKX_HOP_EPIS(0, true)
   QKX_HOP_EPIS(1, false)
@@ -132,15 +138,27 @@ static int hop64(qkx_ctx* c, int basis, bool dag, int epi, const double2* in, do
   return invalid("hop variant");
 }
 
-static int site_op(qkx_ctx* c, int basis, int op, const double2* in, double2* out, double cc, double s) {
-  const int n = 2 * c->Vh;
+// the same on full (both-parity) fields
+static int hop64(qkx_ctx* c, int basis, bool dag, int epi, const double2* in, double2* out, const double2* x,
+                 int out_parity, double a, double cc, double s, double* norm_part = nullptr) {
+  return hop64a(c, basis, dag, epi, F64(in, c->Vh), F64(out, c->Vh), F64(x ? x : in, c->Vh), x && x != in,
+                out_parity, a, cc, s, norm_part);
+}
+
+int site_op_acc(qkx_ctx* c, int basis, int op, SpinorF64 in, SpinorF64 out, int par_first, int npar, double cc,
+                double s) {
+  const int n = npar * c->Vh;
   const int nb = (n + 255) / 256;
   if (basis == 0)
-    k_site_op<0><<<nb, 256, 0, c->st>>>(F64(in, c->Vh), F64(out, c->Vh), 0, 2, op, cc, s);
+    k_site_op<0><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
   else
-    k_site_op<1><<<nb, 256, 0, c->st>>>(F64(in, c->Vh), F64(out, c->Vh), 0, 2, op, cc, s);
+    k_site_op<1><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
+}
+
+static int site_op(qkx_ctx* c, int basis, int op, const double2* in, double2* out, double cc, double s) {
+  return site_op_acc(c, basis, op, F64(in, c->Vh), F64(out, c->Vh), 0, 2, cc, s);
 }
 
 static int zero_parity(qkx_ctx* c, double2* f, int parity) {
@@ -148,9 +166,13 @@ static int zero_parity(qkx_ctx* c, double2* f, int parity) {
   return QKX_OK;
 }
 
-int apply_tm(qkx_ctx* c, const double2* in, double2* out, bool dagger) {
-  const double tw = 2.0 * c->p.kappa * c->p.mu * c->p.twistSign;
+int apply_tm_mu(qkx_ctx* c, const double2* in, double2* out, bool dagger, double mu) {
+  const double tw = 2.0 * c->p.kappa * mu * c->p.twistSign;
   return hop64(c, 0, dagger, EPI_XPAY, in, out, in, -1, -c->p.kappa, dagger ? -tw : tw, 1.0);
+}
+
+int apply_tm(qkx_ctx* c, const double2* in, double2* out, bool dagger) {
+  return apply_tm_mu(c, in, out, dagger, c->p.mu);
 }
 
 // M_xx psi for output parity `par` (0 = EE, 1 = OO) with twist sign `sgn`:

@@ -23,6 +23,8 @@ struct CgScalars {
   double stop[MAX_RHS];
   int active[MAX_RHS];   // 1 while the RHS still iterates
   int iters[MAX_RHS];
+  double aux[MAX_RHS];   // per-RHS results of the batched FP64 residual steps
+  double aux2[MAX_RHS];
 };
 
 template <int NT>

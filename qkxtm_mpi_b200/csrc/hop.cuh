@@ -1,5 +1,6 @@
 // hop.cuh -- the Wilson hopping term D (and D^+) with fused site-local
-// epilogues, one thread per output site, even-odd addressed.
+// epilogues, one thread per output site, even-odd addressed, batched over
+// right-hand sides.
 //
 //   D psi(x)  = sum_mu (1 - g_mu) U_mu(x) psi(x+mu) + (1 + g_mu) U_mu(x-mu)^+ psi(x-mu)
 //   D+ psi(x) = the same with the two projectors exchanged
@@ -10,16 +11,23 @@
 // operator is two parity halves and the even-odd operators are one half each.
 // The antiperiodic time boundary is applied here from the site coordinate
 // (sign bc_sign on t-hops crossing t = Lt-1 -> 0), so compressed links stay SU(3).
+//
+// Grid: blockIdx.x = site_block * nrhs + rhs, so the blocks that work on the
+// same sites for different right-hand sides run back to back and share the
+// links through L2.  When both parities are covered the site blocks alternate
+// parity for the same reason (a link is used forward by its own site and
+// backward by the neighbour of the other parity).
 #pragma once
 #include "qkx_common.cuh"
 
 namespace qkx {
 
 enum Epilogue {
-  EPI_PLAIN = 0,      // out = D psi
-  EPI_XPAY = 1,       // out = a D psi + x + i c g5 x           (tm, tm^+, Wilson, last step of tm_xx)
-  EPI_XPAY_G5 = 2,    // out = g5 (a D psi + x + i c g5 x)      (normal operator through the g5 trick)
-  EPI_TWIST_INV = 3,  // out = s (D psi - i c g5 D psi)          (A^-1 D, first step of tm_xx)
+  EPI_PLAIN = 0,       // out = D psi
+  EPI_XPAY = 1,        // out = a D psi + x + i c g5 x           (tm, tm^+, Wilson, last step of tm_xx)
+  EPI_XPAY_G5 = 2,     // out = g5 (a D psi + x + i c g5 x)      (normal operator through the g5 trick)
+  EPI_TWIST_INV = 3,   // out = s (v - i c g5 v), v = D psi      (A^-1 D, first step of tm_xx)
+  EPI_XPAY_TWINV = 4,  // out = s (v - i c g5 v), v = a D psi + x (odd-parity reconstruction)
 };
 
 template <class SP, class GA>
@@ -29,9 +37,14 @@ struct HopArgs {
   SP x;                // epilogue operand, parity of the output
   GA gauge;
   Geom g;
-  int out_parity;      // 0 or 1; -1 = both parities (grid covers 2*Vh sites)
+  int out_parity;      // 0 or 1; -1 = both parities
   double a, c, s;      // epilogue coefficients
-  double* norm_part;   // if non-null: per-block partial sums of |out|^2
+  double* norm_part;   // if non-null: per-block partial sums of |out|^2, [rhs][site_block]
+  int nrhs;            // right-hand sides in the batch (>= 1)
+  int nblk;            // site blocks per right-hand side
+  const double* cvec;  // optional per-RHS factor on c (twisted mass per RHS)
+  const double* svec;  // optional per-RHS factor on s
+  const int* active;   // optional per-RHS mask; inactive blocks do nothing
 };
 
 template <typename R>
@@ -41,29 +54,29 @@ __device__ __forceinline__ void zero(Spinor<R>& s) {
 }
 
 template <class SP, class GA, typename R, int B, bool DAG, int MU>
-__device__ __forceinline__ void hop_dir(const HopArgs<SP, GA>& A, int par, int cb, const int x[4],
-                                        Spinor<R>& acc) {
+__device__ __forceinline__ void hop_dir(const SP& in, const GA& gauge, const Geom& g, int par, int cb,
+                                        const int x[4], Spinor<R>& acc) {
   constexpr int SF = DAG ? +1 : -1;  // forward projector 1 + SF*g
   HalfSpinor<R> h, uh;
   {
-    int n = cb_neighbour(A.g, x, MU, +1);
-    Spinor<R> s = A.in.load(1 - par, n);
+    int n = cb_neighbour(g, x, MU, +1);
+    Spinor<R> s = in.load(1 - par, n);
     Proj<B, MU, SF>::project(s, h);
-    Link<R> u = A.gauge.load(par, MU, cb);
+    Link<R> u = gauge.load(par, MU, cb);
     mul_link(u, h, uh);
-    if (MU == 3 && A.g.bc_sign < 0 && x[3] == A.g.L[3] - 1) {
+    if (MU == 3 && g.bc_sign < 0 && x[3] == g.L[3] - 1) {
 #pragma unroll
       for (int k = 0; k < 6; k++) uh.c[k / 3][k % 3] = R(-1) * uh.c[k / 3][k % 3];
     }
     Proj<B, MU, SF>::reconstruct(acc, uh);
   }
   {
-    int n = cb_neighbour(A.g, x, MU, -1);
-    Spinor<R> s = A.in.load(1 - par, n);
+    int n = cb_neighbour(g, x, MU, -1);
+    Spinor<R> s = in.load(1 - par, n);
     Proj<B, MU, -SF>::project(s, h);
-    Link<R> u = A.gauge.load(1 - par, MU, n);
+    Link<R> u = gauge.load(1 - par, MU, n);
     mul_link_dag(u, h, uh);
-    if (MU == 3 && A.g.bc_sign < 0 && x[3] == 0) {
+    if (MU == 3 && g.bc_sign < 0 && x[3] == 0) {
 #pragma unroll
       for (int k = 0; k < 6; k++) uh.c[k / 3][k % 3] = R(-1) * uh.c[k / 3][k % 3];
     }
@@ -74,7 +87,7 @@ __device__ __forceinline__ void hop_dir(const HopArgs<SP, GA>& A, int par, int c
 // deterministic two-level sum: each block writes one partial; the caller
 // reduces the partials in a fixed order.
 template <int NT>
-__device__ __forceinline__ void block_partial(double v, double* part) {
+__device__ __forceinline__ void block_partial(double v, double* slot) {
   __shared__ double red[NT / 32];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -84,58 +97,85 @@ __device__ __forceinline__ void block_partial(double v, double* part) {
     double w = threadIdx.x < NT / 32 ? red[threadIdx.x] : 0.0;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) w += __shfl_xor_sync(0xffffffffu, w, o);
-    if (threadIdx.x == 0) part[blockIdx.x] = w;
+    if (threadIdx.x == 0) *slot = w;
   }
+}
+
+template <int B, typename R>
+__device__ __forceinline__ Spinor<R> twist_inv(const Spinor<R>& v, R c, R s) {
+  Spinor<R> g5v = gamma5<B>(v), o;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.c[k / 3][k % 3] = s * (v.c[k / 3][k % 3] - c * phase<1>(g5v.c[k / 3][k % 3]));
+  return o;
 }
 
 template <int NT, class SP, class GA, typename R, int B, bool DAG, int EPI>
 __global__ void __launch_bounds__(NT) hop_kernel(HopArgs<SP, GA> A) {
-  const int idx = blockIdx.x * NT + threadIdx.x;
-  const int n = A.out_parity < 0 ? 2 * A.g.Vh : A.g.Vh;
+  const int rhs = blockIdx.x % A.nrhs;
+  const int blk = blockIdx.x / A.nrhs;
+  double* slot = A.norm_part ? A.norm_part + (size_t)rhs * A.nblk + blk : nullptr;
+  if (A.active && !A.active[rhs]) {
+    if (slot && threadIdx.x == 0) *slot = 0.0;
+    return;
+  }
+  int par, idx;
+  if (A.out_parity < 0) {
+    par = blk & 1;
+    idx = (blk >> 1) * NT + threadIdx.x;
+  } else {
+    par = A.out_parity;
+    idx = blk * NT + threadIdx.x;
+  }
   double nrm = 0.0;
-  if (idx < n) {
-    const int par = A.out_parity < 0 ? (idx >= A.g.Vh ? 1 : 0) : A.out_parity;
-    const int cb = idx - (A.out_parity < 0 ? par * A.g.Vh : 0);
+  if (idx < A.g.Vh) {
+    const SP in = A.in.shift(rhs);
+    const int cb = idx;
     int x[4];
     cb_coords(A.g, cb, par, x);
     Spinor<R> acc;
     zero(acc);
-    hop_dir<SP, GA, R, B, DAG, 0>(A, par, cb, x, acc);
-    hop_dir<SP, GA, R, B, DAG, 1>(A, par, cb, x, acc);
-    hop_dir<SP, GA, R, B, DAG, 2>(A, par, cb, x, acc);
-    hop_dir<SP, GA, R, B, DAG, 3>(A, par, cb, x, acc);
+    hop_dir<SP, GA, R, B, DAG, 0>(in, A.gauge, A.g, par, cb, x, acc);
+    hop_dir<SP, GA, R, B, DAG, 1>(in, A.gauge, A.g, par, cb, x, acc);
+    hop_dir<SP, GA, R, B, DAG, 2>(in, A.gauge, A.g, par, cb, x, acc);
+    hop_dir<SP, GA, R, B, DAG, 3>(in, A.gauge, A.g, par, cb, x, acc);
 
+    const R c = R(A.c * (A.cvec ? A.cvec[rhs] : 1.0));
+    const R s = R(A.s * (A.svec ? A.svec[rhs] : 1.0));
+    const R a = R(A.a);
     Spinor<R> o;
     if constexpr (EPI == EPI_PLAIN) {
       o = acc;
     } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5) {
-      const R a = R(A.a), c = R(A.c);
-      Spinor<R> v = A.x.load(par, cb);
+      Spinor<R> v = A.x.shift(rhs).load(par, cb);
       Spinor<R> g5v = gamma5<B>(v);
 #pragma unroll
-      for (int k = 0; k < 12; k++) {
-        Cx<R> t = phase<1>(g5v.c[k / 3][k % 3]);  // i g5 v
-        o.c[k / 3][k % 3] = a * acc.c[k / 3][k % 3] + (v.c[k / 3][k % 3] + c * t);
-      }
+      for (int k = 0; k < 12; k++)
+        o.c[k / 3][k % 3] = a * acc.c[k / 3][k % 3] + (v.c[k / 3][k % 3] + c * phase<1>(g5v.c[k / 3][k % 3]));
       if constexpr (EPI == EPI_XPAY_G5) o = gamma5<B>(o);
-    } else {  // EPI_TWIST_INV
-      const R c = R(A.c), s = R(A.s);
-      Spinor<R> g5d = gamma5<B>(acc);
+    } else if constexpr (EPI == EPI_TWIST_INV) {
+      o = twist_inv<B>(acc, c, s);
+    } else {  // EPI_XPAY_TWINV
+      Spinor<R> v = A.x.shift(rhs).load(par, cb);
 #pragma unroll
-      for (int k = 0; k < 12; k++) {
-        Cx<R> t = phase<1>(g5d.c[k / 3][k % 3]);
-        o.c[k / 3][k % 3] = s * (acc.c[k / 3][k % 3] - c * t);
-      }
+      for (int k = 0; k < 12; k++) v.c[k / 3][k % 3] = a * acc.c[k / 3][k % 3] + v.c[k / 3][k % 3];
+      o = twist_inv<B>(v, c, s);
     }
-    A.out.store(par, cb, o);
-    if (A.norm_part) {
+    A.out.shift(rhs).store(par, cb, o);
+    if (slot) {
 #pragma unroll
       for (int k = 0; k < 12; k++)
         nrm += double(o.c[k / 3][k % 3].re) * double(o.c[k / 3][k % 3].re) +
                double(o.c[k / 3][k % 3].im) * double(o.c[k / 3][k % 3].im);
     }
   }
-  if (A.norm_part) block_partial<NT>(nrm, A.norm_part);
+  if (slot) block_partial<NT>(nrm, slot);
+}
+
+// launch geometry for hop_kernel: blocks per RHS and total grid
+template <int NT>
+inline int hop_blocks_per_rhs(int Vh, int out_parity) {
+  int per_par = (Vh + NT - 1) / NT;
+  return out_parity < 0 ? 2 * per_par : per_par;
 }
 
 }  // namespace qkx

@@ -1,10 +1,726 @@
-// mixed.cu -- even-odd mixed-precision CG (placeholder until implemented)
+// mixed.cu -- even-odd Schur-complement CG with sloppy spinors and links,
+// FP64 reliable updates, batched over right-hand sides (and twisted masses),
+// the inner iteration replayed from a CUDA graph.
+//
+// System (reference operator Vector::tm, lib/lattice_util.cpp:1925; its Schur
+// form Vector::tm_xx, :2001-2022):
+//   M = [[A, -k D_eo], [-k D_oe, A]],  A = 1 + i c g5,  c = 2 kappa mu twistSign
+//   b^_e = b_e + k D_eo A^-1 b_o
+//   Mh = A - k^2 D_eo A^-1 D_oe   solved on the normal equations Mh^+ Mh x_e = Mh^+ b^_e
+//   Mh^+ = g5 Mh(-c) g5           (the reference builds tm_xxDagTm_xx the same way, :2024)
+//   x_o = A^-1 (b_o + k D_oe x_e)
+// ||b - M x|| = ||b^_e - Mh x_e|| exactly, so the FP64 Schur residual that each
+// reliable update computes is the true residual of the full system; the end of
+// the solve recomputes ||b - M x|| on the full lattice in FP64 as well.
+//
+// Inner iterations (all right-hand sides of the batch in lock-step, per-RHS
+// scalars in device memory, converged RHS masked off):
+//   t_o  = A^-1(c) D_oe p_e                   hop, TWIST_INV
+//   y_e  = g5 (A(c) p_e - k^2 D_eo t_o)        hop, XPAY_G5, |y|^2 = <p, Mh^+Mh p> fused
+//   t_o  = A^-1(-c) D_oe y_e                  hop, TWIST_INV
+//   Ap_e = g5 (A(-c) y_e - k^2 D_eo t_o)       hop, XPAY_G5
+//   alpha = r2 / pAp ; x_s += alpha p ; r_s -= alpha Ap ; r2' = |r_s|^2 ; beta ; p = r_s + beta p
+// p, t, y, Ap are sloppy (FP16 + per-site norm, or FP32); r_s and x_s are FP32.
+// A reliable update (all active right-hand sides together, so the FP64 hops
+// share the links) folds x_s into the FP64 solution and recomputes the
+// residual with the FP64 operator on the 18-real links as the caller gave them.
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <type_traits>
+#include <vector>
+
+#include "blas.cuh"
+#include "hop.cuh"
 #include "qkx_ctx.cuh"
+#include "site_ops.cuh"
+
 namespace qkx {
-int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
-                    double2* const* x, qkx_solve_info* info) {
-  set_error("CG_EO_MIXED not built yet");
-  return QKX_ERR_UNSUPPORTED;
+
+// ---------------------------------------------------------------- precision traits
+struct PHalf {
+  static constexpr int id = QKX_PREC_HALF;
+  using SP = SpinorF16;
+  using GA = GaugeF16x12;
+  using R = float;
+  using AC = SpinorF32;
+  static constexpr double S = 52.0, G = 24.0, delta = 0.1;
+};
+struct PSingle {
+  static constexpr int id = QKX_PREC_SINGLE;
+  using SP = SpinorF32;
+  using GA = GaugeF32x12;
+  using R = float;
+  using AC = SpinorF32;
+  static constexpr double S = 96.0, G = 48.0, delta = 1e-3;
+};
+struct PDouble {
+  static constexpr int id = QKX_PREC_DOUBLE;
+  using SP = SpinorF64;
+  using GA = GaugeF64x18;
+  using R = double;
+  using AC = SpinorF64;
+  static constexpr double S = 192.0, G = 144.0, delta = 1e-30;
+};
+
+// a batch of single-parity fields: data [R][words][Vh] (+ norms [R][Vh] for FP16)
+struct BField {
+  void* d = nullptr;
+  float* n = nullptr;
+};
+
+template <class SPT>
+struct FieldTraits;
+template <>
+struct FieldTraits<SpinorF16> {
+  static constexpr size_t words = 3;
+  static SpinorF16 acc(const BField& f, int par, int Vh) {
+    SpinorF16 s{};
+    uint4* d = (uint4*)f.d;
+    if (par) {
+      s.p1 = d;
+      s.n1 = f.n;
+    } else {
+      s.p0 = d;
+      s.n0 = f.n;
+    }
+    s.Vh = Vh;
+    s.rs = words * Vh;
+    s.rsn = Vh;
+    return s;
+  }
+};
+template <>
+struct FieldTraits<SpinorF32> {
+  static constexpr size_t words = 6;
+  static SpinorF32 acc(const BField& f, int par, int Vh) {
+    SpinorF32 s{};
+    if (par) s.p1 = (float4*)f.d;
+    else s.p0 = (float4*)f.d;
+    s.Vh = Vh;
+    s.rs = words * Vh;
+    return s;
+  }
+};
+template <>
+struct FieldTraits<SpinorF64> {
+  static constexpr size_t words = 12;
+  static SpinorF64 acc(const BField& f, int par, int Vh) {
+    SpinorF64 s{};
+    if (par) s.p1 = (double2*)f.d;
+    else s.p0 = (double2*)f.d;
+    s.Vh = Vh;
+    s.rs = words * Vh;
+    return s;
+  }
+};
+
+// FP64 batch accessor over a raw [R][12][Vh] buffer
+static SpinorF64 B64(double2* base, int par, int Vh) {
+  SpinorF64 s{};
+  if (par) s.p1 = base;
+  else s.p0 = base;
+  s.Vh = Vh;
+  s.rs = 12 * (size_t)Vh;
+  return s;
 }
-void mixed_free(qkx_ctx* c) {}
+// FP64 batch accessor over two [R][12][Vh] buffers holding the even and odd halves
+static SpinorF64 B64full(double2* even, double2* odd, int Vh) {
+  SpinorF64 s{};
+  s.p0 = even;
+  s.p1 = odd;
+  s.Vh = Vh;
+  s.rs = 12 * (size_t)Vh;
+  return s;
+}
+
+template <class SPT>
+static int bfield_alloc(BField& f, int R, int Vh) {
+  using T = FieldTraits<SPT>;
+  if (cudaMalloc(&f.d, T::words * 16 * (size_t)Vh * R) != cudaSuccess) return QKX_ERR_NOMEM;
+  if (std::is_same<SPT, SpinorF16>::value && cudaMalloc(&f.n, sizeof(float) * (size_t)Vh * R) != cudaSuccess)
+    return QKX_ERR_NOMEM;
+  return QKX_OK;
+}
+static void bfield_free(BField& f) {
+  cudaFree(f.d);
+  cudaFree(f.n);
+  f.d = nullptr;
+  f.n = nullptr;
+}
+
+// ---------------------------------------------------------------- kernels
+constexpr int MX_NT = 256;
+constexpr int MX_GRID = 148 * 2;  // blocks per RHS for the streaming kernels
+
+// x_s += alpha p ; r_s -= alpha Ap ; partial |r_s|^2      (one RHS per blockIdx.y)
+template <class SP, class AC, typename R>
+__global__ void __launch_bounds__(MX_NT) k_mx_update_xr(SP p, SP Ap, AC xs, AC rs, const CgScalars* sc,
+                                                        double* part) {
+  const int r = blockIdx.y;
+  double* slot = part + (size_t)r * gridDim.x + blockIdx.x;
+  if (!sc->active[r]) {
+    if (threadIdx.x == 0) *slot = 0.0;
+    return;
+  }
+  const R alpha = R(sc->alpha[r]);
+  const SP pr = p.shift(r), Apr = Ap.shift(r);
+  const AC xr = xs.shift(r), rr = rs.shift(r);
+  double acc = 0.0;
+  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < p.Vh; cb += gridDim.x * MX_NT) {
+    Spinor<R> pv = pr.load(0, cb), av = Apr.load(0, cb), xv = xr.load(0, cb), rv = rr.load(0, cb);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      Cx<R>& X = xv.c[k / 3][k % 3];
+      Cx<R>& Q = rv.c[k / 3][k % 3];
+      X = X + alpha * pv.c[k / 3][k % 3];
+      Q = Q - alpha * av.c[k / 3][k % 3];
+      acc += double(Q.re) * double(Q.re) + double(Q.im) * double(Q.im);
+    }
+    xr.store(0, cb, xv);
+    rr.store(0, cb, rv);
+  }
+  double s = block_sum<MX_NT>(acc);
+  if (threadIdx.x == 0) *slot = s;
+}
+
+// p = r_s + beta p
+template <class SP, class AC, typename R>
+__global__ void __launch_bounds__(MX_NT) k_mx_update_p(SP p, AC rs, const CgScalars* sc) {
+  const int r = blockIdx.y;
+  if (!sc->active[r]) return;
+  const R beta = R(sc->beta[r]);
+  const SP pr = p.shift(r);
+  const AC rr = rs.shift(r);
+  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < p.Vh; cb += gridDim.x * MX_NT) {
+    Spinor<R> pv = pr.load(0, cb), rv = rr.load(0, cb);
+#pragma unroll
+    for (int k = 0; k < 12; k++) pv.c[k / 3][k % 3] = rv.c[k / 3][k % 3] + beta * pv.c[k / 3][k % 3];
+    pr.store(0, cb, pv);
+  }
+}
+
+enum { FIN_AUX = 10, FIN_AUX2 = 11, FIN_AUX_ADD = 12 };
+
+// per-RHS finalize of [R][n] partials (one block per RHS)
+__global__ void __launch_bounds__(256) k_mx_finalize(const double* part, int n, int mode, CgScalars* sc) {
+  const int r = blockIdx.x;
+  if (!sc->active[r]) return;
+  double acc = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) acc += part[(size_t)r * n + i];
+  double s = block_sum<256>(acc);
+  if (threadIdx.x == 0) {
+    if (mode == FIN_PAP) {
+      sc->pAp[r] = s;
+      sc->alpha[r] = sc->r2[r] / s;
+    } else if (mode == FIN_R2) {
+      sc->r2_old[r] = sc->r2[r];
+      sc->r2[r] = s;
+      sc->beta[r] = s / sc->r2_old[r];
+      sc->iters[r] += 1;
+    } else if (mode == FIN_R2_INIT) {
+      sc->r2[r] = s;
+    } else if (mode == FIN_AUX) {
+      sc->aux[r] = s;
+    } else if (mode == FIN_AUX2) {
+      sc->aux2[r] = s;
+    } else {
+      sc->aux[r] += s;
+    }
+  }
+}
+
+// dst(rhs r) = convert(src(rhs r)) for the active RHS of a batch of single-parity fields
+template <class SOUT, typename ROUT>
+__global__ void k_mx_from_f64(SpinorF64 src, SOUT dst, const int* active) {
+  const int r = blockIdx.y;
+  if (active && !active[r]) return;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= src.Vh) return;
+  Spinor<double> v = src.shift(r).load(0, cb);
+  Spinor<ROUT> o;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.c[k / 3][k % 3] = {ROUT(v.c[k / 3][k % 3].re), ROUT(v.c[k / 3][k % 3].im)};
+  dst.shift(r).store(0, cb, o);
+}
+
+// x64(r) += x_s(r) ; x_s(r) = 0   for the active RHS
+template <class AC, typename R>
+__global__ void k_mx_fold(AC xs, SpinorF64 x64, const int* active) {
+  const int r = blockIdx.y;
+  if (active && !active[r]) return;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= x64.Vh) return;
+  const AC xr = xs.shift(r);
+  const SpinorF64 xo = x64.shift(r);
+  Spinor<R> v = xr.load(0, cb);
+  Spinor<double> o = xo.load(0, cb);
+  Spinor<R> z;
+#pragma unroll
+  for (int k = 0; k < 12; k++) {
+    o.c[k / 3][k % 3] = o.c[k / 3][k % 3] + Cx<double>{double(v.c[k / 3][k % 3].re), double(v.c[k / 3][k % 3].im)};
+    z.c[k / 3][k % 3] = {R(0), R(0)};
+  }
+  xo.store(0, cb, o);
+  xr.store(0, cb, z);
+}
+
+// z(r) = a(r) - z(r), partial |z(r)|^2 (batch of single-parity FP64 fields)
+__global__ void __launch_bounds__(MX_NT) k_mx_sub_norm(SpinorF64 a, SpinorF64 z, const int* active, double* part) {
+  const int r = blockIdx.y;
+  double* slot = part + (size_t)r * gridDim.x + blockIdx.x;
+  if (active && !active[r]) {
+    if (threadIdx.x == 0) *slot = 0.0;
+    return;
+  }
+  const SpinorF64 ar = a.shift(r), zr = z.shift(r);
+  double acc = 0.0;
+  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < a.Vh; cb += gridDim.x * MX_NT) {
+    Spinor<double> u = ar.load(0, cb), v = zr.load(0, cb);
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      Cx<double> d = u.c[k / 3][k % 3] - v.c[k / 3][k % 3];
+      v.c[k / 3][k % 3] = d;
+      acc += d.re * d.re + d.im * d.im;
+    }
+    zr.store(0, cb, v);
+  }
+  double s = block_sum<MX_NT>(acc);
+  if (threadIdx.x == 0) *slot = s;
+}
+
+// partial |a(r)|^2 (batch of single-parity FP64 fields)
+__global__ void __launch_bounds__(MX_NT) k_mx_norm(SpinorF64 a, double* part) {
+  const int r = blockIdx.y;
+  const SpinorF64 ar = a.shift(r);
+  double acc = 0.0;
+  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < a.Vh; cb += gridDim.x * MX_NT) {
+    Spinor<double> u = ar.load(0, cb);
+#pragma unroll
+    for (int k = 0; k < 12; k++) acc += u.c[k / 3][k % 3].re * u.c[k / 3][k % 3].re + u.c[k / 3][k % 3].im * u.c[k / 3][k % 3].im;
+  }
+  double s = block_sum<MX_NT>(acc);
+  if (threadIdx.x == 0) part[(size_t)r * gridDim.x + blockIdx.x] = s;
+}
+
+// site-local FP64 op on a batch of single-parity fields
+template <int OP>
+__global__ void k_mx_site(SpinorF64 in, SpinorF64 out, int par, const double* cvec, const double* svec) {
+  const int r = blockIdx.y;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= in.Vh) return;
+  Spinor<double> v = in.shift(r).load(par, cb), o;
+  if constexpr (OP == SITE_GAMMA5) {
+    o = gamma5<0>(v);
+  } else {  // twist inverse with the RHS's own mu
+    o = twist_inv<0>(v, cvec[r], svec[r]);
+  }
+  out.shift(r).store(par, cb, o);
+}
+
+// ---------------------------------------------------------------- solver state
+struct MixedState {
+  int prec = -1;
+  int R = 0;
+  BField p, Ap, t, y, rs, xs;  // sloppy batch fields
+  // FP64 batches [R][12][Vh]
+  double2 *bE = nullptr, *bO = nullptr, *x64 = nullptr, *g5bh = nullptr, *t64 = nullptr, *z64 = nullptr,
+          *r64 = nullptr;
+  double* cvec = nullptr;  // per-RHS 2 kappa mu_r twistSign
+  double* svec = nullptr;  // per-RHS 1 / (1 + (2 kappa mu_r)^2)
+  double* part = nullptr;  // [R][max(nblk, MX_GRID)]
+  cudaGraphExec_t graph = nullptr;
+  int graph_R = 0;
+  double graph_kappa = 0;         // kappa^2 is a kernel argument inside the graph
+  std::vector<cudaEvent_t> gev;   // event pairs captured around the hop kernels
+};
+
+void mixed_free(qkx_ctx* c) {
+  MixedState* m = c->mixed;
+  if (!m) return;
+  cudaStreamSynchronize(c->st);
+  for (BField* f : {&m->p, &m->Ap, &m->t, &m->y, &m->rs, &m->xs}) bfield_free(*f);
+  for (double2* f : {m->bE, m->bO, m->x64, m->g5bh, m->t64, m->z64, m->r64}) cudaFree(f);
+  cudaFree(m->cvec);
+  cudaFree(m->svec);
+  cudaFree(m->part);
+  if (m->graph) cudaGraphExecDestroy(m->graph);
+  for (auto e : m->gev) cudaEventDestroy(e);
+  delete m;
+  c->mixed = nullptr;
+}
+
+template <class P>
+static int mixed_alloc(qkx_ctx* c, int R) {
+  if (c->mixed && c->mixed->prec == P::id && c->mixed->R >= R) return QKX_OK;
+  mixed_free(c);
+  MixedState* m = new MixedState();
+  c->mixed = m;
+  m->prec = P::id;
+  m->R = R;
+  const int Vh = c->Vh;
+  int rc = QKX_OK;
+  for (BField* f : {&m->p, &m->Ap, &m->t, &m->y})
+    if (rc == QKX_OK) rc = bfield_alloc<typename P::SP>(*f, R, Vh);
+  for (BField* f : {&m->rs, &m->xs})
+    if (rc == QKX_OK) rc = bfield_alloc<typename P::AC>(*f, R, Vh);
+  const size_t h64 = sizeof(double2) * 12 * (size_t)Vh * R;
+  for (double2** f : {&m->bE, &m->bO, &m->x64, &m->g5bh, &m->t64, &m->z64, &m->r64})
+    if (rc == QKX_OK && cudaMalloc(f, h64) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  if (rc == QKX_OK && cudaMalloc(&m->cvec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  if (rc == QKX_OK && cudaMalloc(&m->svec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  const int nblk = hop_blocks_per_rhs<128>(Vh, -1);
+  if (rc == QKX_OK && cudaMalloc(&m->part, sizeof(double) * (size_t)R * std::max(nblk, MX_GRID)) != cudaSuccess)
+    rc = QKX_ERR_NOMEM;
+  if (rc != QKX_OK) {
+    mixed_free(c);
+    set_error("mixed solver: device allocation for %d right-hand sides failed", R);
+    return rc;
+  }
+  return QKX_OK;
+}
+
+// ---------------------------------------------------------------- batched hop launcher
+// EPI as in hop.cuh; csign multiplies the per-RHS twist coefficient cvec; with
+// with_s the per-RHS svec scales TWIST_INV epilogues.
+template <class SP, class GA, typename R, int EPI>
+static int hop_batch(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x, int out_parity,
+                     double a, double csign, bool with_s, double* norm_part, int prof_slot) {
+  MixedState* m = c->mixed;
+  HopArgs<SP, GA> A;
+  A.out = out;
+  A.in = in;
+  A.x = x;
+  A.gauge = gauge;
+  A.g = g;
+  A.out_parity = out_parity;
+  A.a = a;
+  A.c = csign;
+  A.s = 1.0;
+  A.norm_part = norm_part;
+  A.nrhs = R_;
+  A.nblk = hop_blocks_per_rhs<128>(c->Vh, out_parity);
+  A.cvec = m->cvec;
+  A.svec = with_s ? m->svec : nullptr;
+  A.active = c->sc->active;
+  if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
+  hop_kernel<128, SP, GA, R, 0, false, EPI><<<A.nblk * R_, 128, 0, c->st>>>(A);
+  QKX_CUDA(cudaGetLastError());
+  if (prof_slot >= 0)
+    QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot + 1], c->st, cudaEventRecordExternal));
+  return QKX_OK;
+}
+
+template <class P>
+struct Sloppy {
+  using SP = typename P::SP;
+  using GA = typename P::GA;
+  using R = typename P::R;
+  using AC = typename P::AC;
+
+  static GA gauge(qkx_ctx* c);
+  static Geom geom(qkx_ctx* c) { return std::is_same<P, PDouble>::value ? c->geom : c->geom_raw; }
+
+  // one inner CG iteration for all right-hand sides (graph-capturable)
+  static int iteration(qkx_ctx* c, int R_, bool prof) {
+    MixedState* m = c->mixed;
+    const int Vh = c->Vh;
+    using FT = FieldTraits<SP>;
+    using FA = FieldTraits<AC>;
+    SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh), Ap = FT::acc(m->Ap, 0, Vh);
+    AC xs = FA::acc(m->xs, 0, Vh), rs = FA::acc(m->rs, 0, Vh);
+    const double k2 = c->p.kappa * c->p.kappa;
+    const int nblk = hop_blocks_per_rhs<128>(Vh, 0);
+    const GA U = gauge(c);
+    const Geom g = geom(c);
+    QKX_TRY((hop_batch<SP, GA, R, EPI_TWIST_INV>(c, R_, U, g, p, t, p, 1, 0.0, +1.0, true, nullptr, prof ? 0 : -1)));
+    QKX_TRY((hop_batch<SP, GA, R, EPI_XPAY_G5>(c, R_, U, g, t, y, p, 0, -k2, +1.0, false, m->part, prof ? 1 : -1)));
+    k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, nblk, FIN_PAP, c->sc);
+    QKX_TRY((hop_batch<SP, GA, R, EPI_TWIST_INV>(c, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr, prof ? 2 : -1)));
+    QKX_TRY((hop_batch<SP, GA, R, EPI_XPAY_G5>(c, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr, prof ? 3 : -1)));
+    dim3 gr(MX_GRID, R_);
+    k_mx_update_xr<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, Ap, xs, rs, c->sc, m->part);
+    k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, MX_GRID, FIN_R2, c->sc);
+    k_mx_update_p<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, rs, c->sc);
+    QKX_CUDA(cudaGetLastError());
+    return QKX_OK;
+  }
+
+  // algorithmic bytes of one of the four inner hops, averaged, per RHS in a batch of R_:
+  // per output site the input and output spinors, 8 links shared by the batch, and
+  // for the two xpay hops one more spinor
+  static double hop_bytes_per_rhs(qkx_ctx* c, int R_) {
+    const double S = P::S, G = P::G, Vh = c->Vh;
+    return Vh * ((2 * S + 8 * G / R_) + (3 * S + 8 * G / R_)) / 2.0;
+  }
+};
+
+template <>
+GaugeF16x12 Sloppy<PHalf>::gauge(qkx_ctx* c) {
+  return GaugeF16x12{c->U12ha, c->U12hb, c->Vh};
+}
+template <>
+GaugeF32x12 Sloppy<PSingle>::gauge(qkx_ctx* c) {
+  return GaugeF32x12{c->U12f, c->Vh};
+}
+template <>
+GaugeF64x18 Sloppy<PDouble>::gauge(qkx_ctx* c) {
+  return GaugeF64x18{c->U18, c->Vh};
+}
+
+// ---------------------------------------------------------------- batched FP64 pieces
+using H18 = GaugeF64x18;
+
+// out(r) = g5 Mh(csign * c_r) v(r) for the active RHS, through t64; optional |out|^2 partials
+static int schur64_g5_batch(qkx_ctx* c, int R_, double csign, double2* v, double2* out, double* norm_part) {
+  MixedState* m = c->mixed;
+  const int Vh = c->Vh;
+  const double k = c->p.kappa;
+  const H18 U{c->U18, Vh};
+  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_TWIST_INV>(c, R_, U, c->geom, B64(v, 0, Vh), B64(m->t64, 1, Vh),
+                                                            B64(v, 0, Vh), 1, 0.0, csign, true, nullptr, -1)));
+  return hop_batch<SpinorF64, H18, double, EPI_XPAY_G5>(c, R_, U, c->geom, B64(m->t64, 1, Vh), B64(out, 0, Vh),
+                                                        B64(v, 0, Vh), 0, -k * k, csign, false, norm_part, -1);
+}
+
+template <class P>
+static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
+                             double2* const* x, qkx_solve_info* info) {
+  using SL = Sloppy<P>;
+  using SP = typename P::SP;
+  using AC = typename P::AC;
+  using R = typename P::R;
+  using FT = FieldTraits<SP>;
+  using FA = FieldTraits<AC>;
+  QKX_TRY(mixed_alloc<P>(c, nrhs));
+  MixedState* m = c->mixed;
+  const int Vh = c->Vh;
+  const size_t n12 = 12 * (size_t)Vh;
+  const size_t hb = sizeof(double2) * n12;
+  const double k = c->p.kappa, ts = c->p.twistSign;
+  const double delta = sp->reliable_delta > 0 ? std::max(1e-12, std::min(0.5, sp->reliable_delta)) : P::delta;
+  const int nblk = hop_blocks_per_rhs<128>(Vh, 0);
+  const int cgrid = (Vh + 255) / 256;
+  const dim3 cg2(cgrid, nrhs), bg2(MX_GRID, nrhs);
+  const H18 U18{c->U18, Vh};
+
+  std::vector<double> mus(nrhs), cv(nrhs), sv(nrhs);
+  for (int i = 0; i < nrhs; i++) {
+    mus[i] = sp->mu ? sp->mu[i] : c->p.mu;
+    cv[i] = 2.0 * k * mus[i] * ts;
+    sv[i] = 1.0 / (1.0 + (2.0 * k * mus[i]) * (2.0 * k * mus[i]));
+  }
+  CgScalars* sh = c->sc_h;
+  memset(sh, 0, sizeof(CgScalars));
+  for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
+
+  QKX_CUDA(cudaEventRecord(c->t0, c->st));
+  QKX_CUDA(cudaMemcpyAsync(m->cvec, cv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemcpyAsync(m->svec, sv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemcpyAsync(c->sc, sh, sizeof(CgScalars), cudaMemcpyHostToDevice, c->st));
+
+  // --- set-up, batched FP64: gather b, |b|^2; b^_e = b_e + k D_eo A^-1 b_o; g5 b^_e; r = Mh^+ b^_e
+  for (int i = 0; i < nrhs; i++) {
+    QKX_CUDA(cudaMemcpyAsync(m->bE + i * n12, b[i], hb, cudaMemcpyDeviceToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(m->bO + i * n12, b[i] + n12, hb, cudaMemcpyDeviceToDevice, c->st));
+  }
+  k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), m->part);
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+  k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), m->part);
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+  // t_o = A^-1 b_o
+  k_mx_site<SITE_TWIST_INV><<<cg2, 256, 0, c->st>>>(B64(m->bO, 1, Vh), B64(m->t64, 1, Vh), 1, m->cvec, m->svec);
+  QKX_CUDA(cudaGetLastError());
+  // z = b_e + k D_eo t_o = b^_e, |b^|^2 -> aux2 ; g5bh = g5 b^_e
+  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY>(c, nrhs, U18, c->geom, B64(m->t64, 1, Vh), B64(m->z64, 0, Vh),
+                                                       B64(m->bE, 0, Vh), 0, k, 0.0, false, m->part, -1)));
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_AUX2, c->sc);
+  k_mx_site<SITE_GAMMA5><<<cg2, 256, 0, c->st>>>(B64(m->z64, 0, Vh), B64(m->g5bh, 0, Vh), 0, nullptr, nullptr);
+  // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2
+  QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part));
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_R2_INIT, c->sc);
+  QKX_CUDA(cudaMemsetAsync(m->x64, 0, hb * nrhs, c->st));
+  QKX_CUDA(cudaMemsetAsync(m->xs.d, 0, FA::words * 16 * (size_t)Vh * nrhs, c->st));
+  k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
+  k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+  QKX_CUDA(cudaGetLastError());
+  QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+
+  std::vector<double> bnorm2(nrhs), r2ru(nrhs), ratio(nrhs, 1.0);
+  std::vector<int> active(nrhs, 1);
+  for (int i = 0; i < nrhs; i++) {
+    bnorm2[i] = sh->aux[i];
+    r2ru[i] = sh->r2[i];
+    ratio[i] = sh->r2[i] > 0 ? sh->aux2[i] / sh->r2[i] : 1.0;  // ||rhat||^2 / ||Mh^+ rhat||^2 at x = 0
+    if (bnorm2[i] == 0.0 || sh->r2[i] == 0.0) active[i] = 0;
+    sh->active[i] = active[i];
+  }
+  QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+
+  // --- graph of one inner iteration
+  const bool prof = c->prof != 0;
+  if (prof && m->gev.size() < 8) {
+    for (int e = (int)m->gev.size(); e < 8; e++) {
+      cudaEvent_t ev;
+      QKX_CUDA(cudaEventCreate(&ev));
+      m->gev.push_back(ev);
+    }
+  }
+  const bool graphs = sp->use_graphs != 0;
+  if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || !graphs || prof)) {
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+  if (graphs && !m->graph) {
+    cudaGraph_t gr;
+    QKX_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    int rc = SL::iteration(c, nrhs, prof);
+    cudaError_t e = cudaStreamEndCapture(c->st, &gr);
+    if (rc != QKX_OK) return rc;
+    if (e != cudaSuccess) {
+      set_error("graph capture: %s", cudaGetErrorString(e));
+      return QKX_ERR_CUDA;
+    }
+    QKX_CUDA(cudaGraphInstantiate(&m->graph, gr, 0));
+    cudaGraphDestroy(gr);
+    m->graph_R = nrhs;
+    m->graph_kappa = c->p.kappa;
+  }
+
+  const int maxIter = sp->maxIter;
+  const double target = 0.9 * sp->tol;
+  int iter = 0, n_ru = 0, since = 0;
+  while (iter < maxIter) {
+    int nact = 0;
+    for (int i = 0; i < nrhs; i++) nact += active[i];
+    if (!nact) break;
+    if (m->graph) {
+      QKX_CUDA(cudaGraphLaunch(m->graph, c->st));
+    } else {
+      QKX_TRY(SL::iteration(c, nrhs, prof));
+    }
+    iter++;
+    since++;
+    QKX_CUDA(cudaMemcpyAsync(sh->r2, c->sc->r2, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, c->st));
+    QKX_CUDA(cudaStreamSynchronize(c->st));
+    if (prof) {
+      for (int h = 0; h < 4; h++) {
+        float ms = 0;
+        QKX_CUDA(cudaEventElapsedTime(&ms, m->gev[2 * h], m->gev[2 * h + 1]));
+        c->prof_ms += ms;
+        c->prof_launches++;
+        c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs) * nact;
+      }
+    }
+    // reliable update of every active RHS when one of them asks for it
+    bool ru = since >= 200;
+    for (int i = 0; i < nrhs; i++) {
+      if (!active[i]) continue;
+      const double r2s = sh->r2[i];
+      if (!(r2s == r2s) || isinf(r2s)) {
+        set_error("mixed CG: r2 of right-hand side %d became %g at iteration %d", i, r2s, iter);
+        return QKX_ERR_NAN;
+      }
+      if (r2s < delta * delta * r2ru[i] || r2s * ratio[i] <= target * target * bnorm2[i]) ru = true;
+    }
+    if (!ru) continue;
+    n_ru++;
+    since = 0;
+    // x64 += x_s ; z = g5 b^ - g5 Mh x64 = g5 rhat ; r = Mh^+ rhat
+    k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+    QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
+    k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_AUX2, c->sc);
+    QKX_CUDA(cudaGetLastError());
+    QKX_CUDA(cudaMemcpyAsync(sh->aux, c->sc->aux, 2 * sizeof(double) * MAX_RHS, cudaMemcpyDeviceToHost, c->st));
+    QKX_CUDA(cudaStreamSynchronize(c->st));
+    for (int i = 0; i < nrhs; i++) {
+      if (!active[i]) continue;
+      const double rhat2 = sh->aux[i], r2 = sh->aux2[i];
+      if (rhat2 <= target * target * bnorm2[i] || r2 == 0.0) {
+        active[i] = 0;
+        sh->active[i] = 0;
+        continue;
+      }
+      ratio[i] = rhat2 / r2;
+      r2ru[i] = r2;
+      sh->r2[i] = r2;
+    }
+    // restart the sloppy residual from the FP64 one for the RHS that go on
+    QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+    k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
+    QKX_CUDA(cudaGetLastError());
+  }
+  int rc = QKX_OK;
+  int nact = 0;
+  for (int i = 0; i < nrhs; i++) nact += active[i];
+  if (nact) rc = QKX_ERR_NOT_CONVERGED;
+
+  // --- odd parity and the FP64 true residual of the full system, batched
+  for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
+  QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+  if (nact)  // fold what the unconverged RHS accumulated since their last update
+    k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+  // x_o = A^-1 (b_o + k D_oe x_e) into t64
+  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY_TWINV>(c, nrhs, U18, c->geom, B64(m->x64, 0, Vh),
+                                                             B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0, true,
+                                                             nullptr, -1)));
+  // M x on the full lattice (even half in x64, odd half in t64) into (z64, r64)
+  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY>(c, nrhs, U18, c->geom, B64full(m->x64, m->t64, Vh),
+                                                       B64full(m->z64, m->r64, Vh), B64full(m->x64, m->t64, Vh), -1,
+                                                       -k, 1.0, false, nullptr, -1)));
+  k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), B64(m->z64, 0, Vh), nullptr, m->part);
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+  k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), B64(m->r64, 0, Vh), nullptr, m->part);
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+  QKX_CUDA(cudaGetLastError());
+  for (int i = 0; i < nrhs; i++) {
+    QKX_CUDA(cudaMemcpyAsync(x[i], m->x64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(x[i] + n12, m->t64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
+  }
+  QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
+  QKX_CUDA(cudaEventRecord(c->t1, c->st));
+  QKX_CUDA(cudaEventSynchronize(c->t1));
+  double worst = 0.0;
+  int it = 0;
+  for (int i = 0; i < nrhs; i++) {
+    double rel = bnorm2[i] > 0 ? sqrt(sh->aux[i] / bnorm2[i]) : 0.0;
+    worst = std::max(worst, rel);
+    it = std::max(it, sh->iters[i]);
+  }
+  if (rc == QKX_OK && worst > sp->tol) rc = QKX_ERR_NOT_CONVERGED;
+  if (info) {
+    info->iterations = it;
+    info->reliable_updates = n_ru;
+    info->converged = rc == QKX_OK;
+    info->true_residual = worst;
+    info->normal_residual = 0.0;
+    float ms = 0;
+    cudaEventElapsedTime(&ms, c->t0, c->t1);
+    info->seconds = ms * 1e-3;
+  }
+  if (rc == QKX_ERR_NOT_CONVERGED)
+    set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
+  return rc;
+}
+
+int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b, double2* const* x,
+                    qkx_solve_info* info) {
+  if (sp->sloppy_precision == QKX_PREC_DOUBLE) return invert_eo_mixed_t<PDouble>(c, sp, nrhs, b, x, info);
+  if (!c->compressible) {
+    set_error("mixed precision needs SU(3) links (12-real reconstruction); these links are not unitary "
+              "to 1e-6 (max |UU^+-1| = %g)", c->link_unitarity);
+    return QKX_ERR_UNSUPPORTED;
+  }
+  if (sp->sloppy_precision == QKX_PREC_SINGLE) return invert_eo_mixed_t<PSingle>(c, sp, nrhs, b, x, info);
+  if (sp->sloppy_precision == QKX_PREC_HALF) return invert_eo_mixed_t<PHalf>(c, sp, nrhs, b, x, info);
+  set_error("invalid argument: sloppy_precision");
+  return QKX_ERR_INVALID;
+}
+
 }  // namespace qkx

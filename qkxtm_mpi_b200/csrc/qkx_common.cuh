@@ -245,6 +245,13 @@ struct SpinorF64 {
   double2* p0;
   double2* p1;
   int Vh;
+  size_t rs = 0;  // words between consecutive right-hand sides of a batch
+  __device__ __forceinline__ SpinorF64 shift(int r) const {
+    SpinorF64 o = *this;
+    if (p0) o.p0 = p0 + rs * r;
+    if (p1) o.p1 = p1 + rs * r;
+    return o;
+  }
   __device__ __forceinline__ Spinor<double> load(int parity, int cb) const {
     const double2* b = (parity ? p1 : p0) + cb;
     Spinor<double> s;
@@ -267,6 +274,13 @@ struct SpinorF32 {
   float4* p0;
   float4* p1;
   int Vh;
+  size_t rs = 0;
+  __device__ __forceinline__ SpinorF32 shift(int r) const {
+    SpinorF32 o = *this;
+    if (p0) o.p0 = p0 + rs * r;
+    if (p1) o.p1 = p1 + rs * r;
+    return o;
+  }
   __device__ __forceinline__ Spinor<float> load(int parity, int cb) const {
     const float4* b = (parity ? p1 : p0) + cb;
     Spinor<float> s;
@@ -296,6 +310,16 @@ struct SpinorF16 {
   float* n0;
   float* n1;
   int Vh;
+  size_t rs = 0;   // uint4 words between right-hand sides
+  size_t rsn = 0;  // norms between right-hand sides
+  __device__ __forceinline__ SpinorF16 shift(int r) const {
+    SpinorF16 o = *this;
+    if (p0) o.p0 = p0 + rs * r;
+    if (p1) o.p1 = p1 + rs * r;
+    if (n0) o.n0 = n0 + rsn * r;
+    if (n1) o.n1 = n1 + rsn * r;
+    return o;
+  }
   __device__ __forceinline__ Spinor<float> load(int parity, int cb) const {
     const uint4* b = (parity ? p1 : p0) + cb;
     float n = __ldg((parity ? n1 : n0) + cb);
@@ -318,6 +342,9 @@ struct SpinorF16 {
     float m = 0.f;
 #pragma unroll
     for (int k = 0; k < 12; k++) m = fmaxf(m, fmaxf(fabsf(s.c[k / 3][k % 3].re), fabsf(s.c[k / 3][k % 3].im)));
+    // below FLT_MIN the reciprocal would overflow; such a site is stored as zero
+    // (its entries are negligible next to any spinor the solver works with)
+    if (!(m >= 1.17549435e-38f)) m = 0.f;
     float inv = m > 0.f ? 1.f / m : 0.f;
     uint4* b = (parity ? p1 : p0) + cb;
 #pragma unroll

@@ -92,6 +92,18 @@ int finalize(qkx_ctx* c, int nparts, int mode, double* dst, int rhs);
 int run_op(qkx_ctx* c, int op, const double2* in, double2* out);
 // M (tm) or M^+ on full FP64 fields with the 18-real links, fused twist
 int apply_tm(qkx_ctx* c, const double2* in, double2* out, bool dagger);
+int apply_tm_mu(qkx_ctx* c, const double2* in, double2* out, bool dagger, double mu);
+// FP64 hopping kernel on accessors (one parity or both), see hop.cuh for the epilogues
+int hop64a(qkx_ctx* c, int basis, bool dag, int epi, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_distinct,
+           int out_parity, double a, double cc, double s, double* norm_part);
+// site-local operator (site_ops.cuh) on parities [par_first, par_first + npar)
+int site_op_acc(qkx_ctx* c, int basis, int op, SpinorF64 in, SpinorF64 out, int par_first, int npar, double cc,
+                double s);
+// FP64 accessor for a single-parity field [12][Vh]
+inline SpinorF64 H64(const double2* base, int parity, int Vh) {
+  double2* b = const_cast<double2*>(base);
+  return parity ? SpinorF64{nullptr, b, Vh} : SpinorF64{b, nullptr, Vh};
+}
 
 // mixed-precision solver entry (mixed.cu)
 int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,

@@ -1,0 +1,143 @@
+"""GPU tests of the solvers: every solve must reach ||b - M x|| / ||b|| <= 1e-10
+recomputed in FP64 by the oracle, for the plain FP64 method and the even-odd
+mixed-precision method (half, single, double sloppy), batched right-hand
+sides, several twisted masses in one batch, and the error paths."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-10
+
+
+def true_res(O, L, U, x, b, kappa, mu, ts=1):
+    r = b - O.apply("tm", L, U, x, kappa, mu, ts)
+    return float(np.sqrt(np.sum(r * r) / np.sum(b * b)))
+
+
+@pytest.fixture(scope="module")
+def setup8(qkx, oracle):
+    L = (8, 8, 8, 16)
+    U = oracle.apply_bc(L, oracle.gauge_random(L, 0.3, 4321), -1)
+    lat = qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004, twistSign=1))
+    lat.load_gauge(U)
+    yield L, U, lat
+    lat.close()
+
+
+@pytest.mark.parametrize("prec", ["half", "single", "double"])
+def test_eo_mixed_reaches_true_residual(qkx, oracle, setup8, prec):
+    L, U, lat = setup8
+    p = {"half": qkx.PREC_HALF, "single": qkx.PREC_SINGLE, "double": qkx.PREC_DOUBLE}[prec]
+    b = oracle.spinor_gaussian(L, 11)
+    xs, info = lat.invert([b], method=qkx.SOLVER_CG_EO_MIXED, precision=p, tol=TOL)
+    tr = true_res(oracle, L, U, xs[0], b, 0.1615, 0.004)
+    assert tr <= TOL, tr
+    assert info.converged == 1 and info.true_residual <= TOL
+    np.testing.assert_allclose(info.true_residual, tr, rtol=1e-2)
+    # same solution as the reference's own method (oracle FP64 CG on M^+M)
+    Mdb = oracle.apply("tm_dag", L, U, b, 0.1615, 0.004)
+    x_ref, _, _ = oracle.cg(L, U, Mdb, 0.1615, 0.004, tol=1e-12, maxIter=2000)
+    assert rel(xs[0], x_ref) < 1e-8
+
+
+def test_eo_mixed_matches_fp64_method(qkx, oracle, setup8):
+    L, U, lat = setup8
+    b = oracle.spinor_gaussian(L, 12)
+    x1, i1 = lat.invert([b], method=qkx.SOLVER_CG_FP64, tol=TOL)
+    x2, i2 = lat.invert([b], method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_HALF, tol=TOL)
+    assert rel(x2[0], x1[0]) < 1e-8
+    # the even-odd system converges in fewer iterations than the full normal equations
+    assert i2.iterations < i1.iterations
+
+
+def test_multi_rhs_batch_point_sources(qkx, oracle, setup8):
+    """12 spin-colour point sources in one batch; each one to 1e-10."""
+    L, U, lat = setup8
+    bs = [oracle.spinor_point(L, (0, 0, 0, 0), s, c) for s in range(4) for c in range(3)]
+    xs, info = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_HALF, tol=TOL)
+    assert info.converged == 1
+    for b, x in zip(bs, xs):
+        assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
+
+
+def test_batch_equals_single_solves(qkx, oracle, setup8):
+    L, U, lat = setup8
+    bs = [oracle.spinor_gaussian(L, 20 + i) for i in range(3)]
+    xb, _ = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_SINGLE, tol=TOL)
+    for b, x in zip(bs, xb):
+        xs, _ = lat.invert([b], method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_SINGLE, tol=TOL)
+        assert rel(x, xs[0]) < 1e-8
+
+
+def test_multi_mass_batch(qkx, oracle, setup8):
+    """Several twisted masses in one batch: each RHS solves its own M(mu_i)."""
+    import ctypes as C
+    L, U, lat = setup8
+    mus = [0.0015, 0.004, 0.01]
+    bs = [oracle.spinor_gaussian(L, 30 + i) for i in range(3)]
+    xs = [np.empty_like(b) for b in bs]
+    n = len(bs)
+    arr = (C.c_double * n)(*mus)
+    sp = qkx.SolverParams(qkx.SOLVER_CG_EO_MIXED, qkx.PREC_HALF, TOL, 10000, 0.0, 1,
+                          C.cast(arr, C.POINTER(C.c_double)))
+    info = qkx.SolveInfo()
+    bp = (C.c_void_p * n)(*[b.ctypes.data for b in bs])
+    xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+    qkx.check(qkx.lib().qkx_invert(lat.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
+    for mu, b, x in zip(mus, bs, xs):
+        assert true_res(oracle, L, U, x, b, 0.1615, mu) <= TOL
+
+
+def test_graph_and_eager_agree_bitwise(qkx, oracle, setup8):
+    L, U, lat = setup8
+    b = oracle.spinor_gaussian(L, 40)
+    xg, ig = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, use_graphs=1)
+    xe, ie = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, use_graphs=0)
+    assert ig.iterations == ie.iterations
+    assert np.array_equal(xg[0], xe[0])
+
+
+def test_twist_sign_and_periodic_links(qkx, oracle):
+    L = (4, 4, 4, 8)
+    Uraw = oracle.gauge_random(L, 0.3, 99)
+    b = oracle.spinor_gaussian(L, 98)
+    for ts, bc in ((-1, -1), (1, 1)):
+        with qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.16, mu=0.01, twistSign=ts, boundaryT=bc)) as lat:
+            lat.load_gauge(Uraw, qkx.LINKS_APPLY_BC)
+            Uop = oracle.apply_bc(L, Uraw, bc)
+            xs, _ = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL)
+            assert true_res(oracle, L, Uop, xs[0], b, 0.16, 0.01, ts) <= TOL
+
+
+def test_zero_source_gives_zero_solution(qkx, oracle, setup8):
+    L, U, lat = setup8
+    b = np.zeros((oracle.volume(L), 4, 3, 2))
+    xs, info = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL)
+    assert not np.any(xs[0])
+    assert info.converged == 1
+
+
+def test_non_su3_links_refuse_mixed_precision(qkx, oracle):
+    L = (4, 4, 4, 8)
+    U = oracle.gauge_random(L, 0.3, 5) * 1.01
+    with qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.16, mu=0.01)) as lat:
+        lat.load_gauge(U)
+        with pytest.raises(qkx.QkxError) as e:
+            lat.invert([oracle.spinor_gaussian(L, 1)], precision=qkx.PREC_HALF, tol=TOL)
+        assert e.value.code == qkx.ERR_UNSUPPORTED
+        # the FP64 methods still work on them
+        xs, _ = lat.invert([oracle.spinor_gaussian(L, 1)], precision=qkx.PREC_DOUBLE, tol=TOL)
+        assert true_res(oracle, L, U, xs[0], oracle.spinor_gaussian(L, 1), 0.16, 0.01) <= TOL
+
+
+def test_maxiter_reports_not_converged(qkx, oracle, setup8):
+    L, U, lat = setup8
+    b = oracle.spinor_gaussian(L, 50)
+    xs, info = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, maxIter=5, strict=False)
+    assert info.converged == 0
+    with pytest.raises(qkx.QkxError) as e:
+        lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, maxIter=5)
+    assert e.value.code == qkx.ERR_NOT_CONVERGED
