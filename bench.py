@@ -1,0 +1,369 @@
+#!/usr/bin/env python
+"""Benchmark of the twisted-mass Dslash / CG hot path on B200.
+
+Workload (the north-star configuration): 32^3 x 64 lattice, synthetic links
+U = exp(i 0.3 H) (seeded), antiperiodic time boundary, kappa = 0.1615,
+mu = 0.0015, the 12 spin-colour point sources at the origin, every source
+solved to a true residual ||b - M x|| / ||b|| <= 1e-10 recomputed in FP64.
+
+A step is one solve of all 12 sources (time to solution).  `value` is the
+device time of a step with inputs resident in HBM (even-odd mixed-precision
+CG, all sources in one batch, CUDA-graph iterations); `e2e` is the same step
+through the host-buffer C ABI (qkx_load_gauge + qkx_invert from page-locked
+host memory, solutions read back).  The plain FP64 CG of the reference's
+algorithm on the same GPU is timed beside it (`plain_fp64_s`).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank solves its own 12 sources (point sources on
+time slice 2*rank): weak scaling, no data-path collective; `value` is the
+max over ranks of the per-step device time.
+`--impl reference` times the reference's own CPU code (compiled from its
+sources, oracle/_ref) on the host cores instead.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+L = (32, 32, 32, 64)
+KAPPA, MU, EPS, SEED, NSRC, TOL = 0.1615, 0.0015, 0.3, 1234, 12, 1e-10
+WORKLOAD = (f"twisted-mass CG, {L[0]}^3x{L[3]}, {NSRC} spin-colour point sources, "
+            f"kappa={KAPPA}, mu={MU}, eps={EPS}, antiperiodic t, true residual <= {TOL:g}")
+METRIC = "CG time-to-solution at 1e-10, 12 point sources, 32^3x64 (mu=0.0015)"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
+            int(os.environ.get("LOCAL_RANK", 0)))
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of one GPU during a region (200 ms period)."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, local_rank: int):
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        ids = [v.strip() for v in vis.split(",")] if vis else None
+        self.gpu = ids[local_rank] if ids and local_rank < len(ids) else str(local_rank)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        rows = []
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 8:
+                continue
+            try:
+                rows.append((float(f[0]), float(f[1]), f[4:8]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, fl in rows for i, v in enumerate(fl) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in rows), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def point_sources(np, t_src: int):
+    V = L[0] * L[1] * L[2] * L[3]
+    site = L[0] * L[1] * L[2] * t_src
+    out = []
+    for s in range(4):
+        for c in range(3):
+            b = np.zeros((V, 4, 3, 2))
+            b[site, s, c, 0] = 1.0
+            out.append(b)
+    return out
+
+
+# --------------------------------------------------------------------------- ours
+def run_ours(args):
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    import qkxtm_mpi_b200 as Q
+
+    rank, world, local = env_rank()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    prec = {"half": Q.PREC_HALF, "single": Q.PREC_SINGLE, "double": Q.PREC_DOUBLE}[args.precision]
+    V = L[0] * L[1] * L[2] * L[3]
+
+    lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, twistSign=1, boundaryT=-1, tol=TOL,
+                                  maxIter=5000), device=local)
+    lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
+    t_src = (2 * rank) % L[3]
+    srcs = point_sources(np, t_src)
+    bd = [lat.field(b) for b in srcs]
+    xd = [lat.field() for _ in srcs]
+    stream = torch.cuda.ExternalStream(lat.stream())
+
+    def solve():
+        info = lat.invert_dev(bd, xd, method=Q.SOLVER_CG_EO_MIXED, precision=prec, tol=TOL,
+                              maxIter=5000)
+        if not (info.converged and info.true_residual <= TOL):
+            raise RuntimeError(f"solve did not converge: {info.as_dict()}")
+        return info
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        solve()
+    lat.sync()
+
+    # ---- timed region: inputs resident in HBM
+    barrier()
+    torch.cuda.synchronize()
+    lat.profile_reset()
+    lat.profile(True)
+    k0 = lat.kernel_launches()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    infos = []
+    with ClockSampler(local) as clk:
+        e0.record(stream)
+        for _ in range(args.steps):
+            infos.append(solve())
+        e1.record(stream)
+        torch.cuda.synchronize()
+    barrier()
+    launches = lat.kernel_launches() - k0
+    hop_n, hop_ms, hop_bytes = lat.profile_read()
+    lat.profile(False)
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    step_s = ms / 1e3 / args.steps
+
+    # ---- end to end through the host-buffer C ABI
+    Uh = Q.pinned_array((V, 4, 3, 3, 2))
+    Uh[...] = lat.download_gauge()
+    bh = [Q.pinned_array((V, 4, 3, 2)) for _ in srcs]
+    for h, b in zip(bh, srcs):
+        h[...] = b
+    xh = [Q.pinned_array((V, 4, 3, 2)) for _ in srcs]
+
+    def e2e_step():
+        lat.load_gauge(Uh, Q.LINKS_AS_GIVEN)
+        _, info = lat.invert(bh, method=Q.SOLVER_CG_EO_MIXED, precision=prec, tol=TOL, maxIter=5000,
+                             out=xh)
+        return info
+
+    e2e_step()
+    n_e2e = max(1, min(args.steps, 3))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(n_e2e):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    if world > 1:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    h2d = Uh.nbytes + sum(b.nbytes for b in bh)
+    d2h = sum(x.nbytes for x in xh)
+
+    # ---- the plain FP64 method (the reference's algorithm) on the same GPU
+    plain = None
+    if not args.no_plain:
+        torch.cuda.synchronize()
+        pinfo = lat.invert_dev(bd, xd, method=Q.SOLVER_CG_FP64, tol=TOL, maxIter=5000)
+        plain = {"seconds": pinfo.seconds, "iterations": pinfo.iterations,
+                 "true_residual": pinfo.true_residual}
+
+    # ---- CPU baseline (rank 0, N = 1)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import cpu_baseline as CB
+        iters = plain["iterations"] if plain else None
+        cb = CB.run(L, KAPPA, MU, EPS, SEED, n_sources=NSRC, n_iter=1, iters_full=iters,
+                    links=np.array(Uh))
+        cpu = {"value": cb["value"], "unit": "s", "cores": cb["cores"], "kind": cb["kind"],
+               "sample": cb["sample"]}
+
+    if world > 1:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    peak, peak_src = measured_peak_hbm()
+    avg_launch_ms = hop_ms / max(hop_n, 1)
+    bytes_per_launch = hop_bytes / max(hop_n, 1)
+    achieved = bytes_per_launch / (avg_launch_ms * 1e-3) / 1e9 if hop_n else None
+    traffic = None
+    tfile = os.path.join(ROOT, "profiles", "hop_traffic.json")
+    if os.path.exists(tfile):
+        with open(tfile) as f:
+            tj = json.load(f)
+        key = args.precision
+        if key in tj:
+            # ncu DRAM bytes per output site per RHS of the captured launch, scaled to this launch
+            traffic = tj[key]["dram_bytes_per_site_rhs"] * (V // 2) * NSRC
+    it = max(i.iterations for i in infos)
+    line = {
+        "metric": METRIC,
+        "value": step_s,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": step_s * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic (seeded exp(i eps H) links, point sources)",
+        "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, L)), "sources_per_gpu": NSRC,
+                   "solver": "even-odd CG, all sources in one batch, CUDA-graph iterations",
+                   "storage": {"half": "fp16 spinors + 12-real fp16 links",
+                               "single": "fp32 spinors + 12-real fp32 links",
+                               "double": "fp64"}[args.precision],
+                   "accumulate": "fp32 inner, fp64 reliable updates / solution / residual checks",
+                   "l2": "inputs larger than L2 (links alone 201 MB fp16, spinor batches > 600 MB)",
+                   "parallelism": f"replicas x{world} (independent sources per GPU)"},
+        "iterations": it,
+        "reliable_updates": max(i.reliable_updates for i in infos),
+        "true_residual_max": max(i.true_residual for i in infos),
+        "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "gpu_launches": launches,
+        "roofline": {
+            "kernel": f"hop_kernel<{args.precision}, 12-real links, {NSRC} RHS batch>",
+            "bound": "hbm",
+            "achieved": achieved,
+            "peak": peak,
+            "peak_source": peak_src,
+            "unit": "GB/s",
+            "frac": (achieved / peak) if achieved else None,
+            "traffic": traffic,
+            "launches": hop_n,
+            "avg_launch_ms": avg_launch_ms,
+            "algorithmic_bytes_per_launch": bytes_per_launch,
+        },
+        "clocks": clk.summary(),
+    }
+    if plain:
+        line["plain_fp64_s"] = plain["seconds"]
+        line["plain_fp64_iterations"] = plain["iterations"]
+        line["speedup_vs_plain_fp64"] = plain["seconds"] / step_s
+    if cpu:
+        line["cpu_baseline"] = cpu
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------- reference
+def run_reference(args):
+    rank, world, _ = env_rank()
+    if rank != 0:
+        return
+    import numpy as np
+    from oracle import cpu_baseline as CB
+    from oracle import oracle as O
+
+    O.build(ref=True)
+    links = O.apply_bc(L, O.gauge_random(L, EPS, SEED), -1)
+    # iterations of the reference's own stopping rule, from a small lattice
+    iters = CB.iterations_to_converge((8, 8, 8, 16), KAPPA, MU, EPS, SEED)
+    vals, last = [], None
+    for i in range(args.warmup + args.steps):
+        last = CB.run(L, KAPPA, MU, EPS, SEED, n_sources=NSRC, n_iter=1, iters_full=iters, links=links)
+        if i >= args.warmup:
+            vals.append(last["value"])
+    value = statistics.median(vals)
+    line = {
+        "impl": "reference",
+        "metric": METRIC,
+        "value": value,
+        "unit": "s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": value * 1e3,
+        "higher_is_better": False,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded exp(i eps H) links, point sources)",
+        "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, L)), "sources_per_gpu": NSRC,
+                   "solver": "reference CG::operator() on M^+M (lib/solvers.cpp), FP64, host cores"},
+        "cpu_baseline": {"value": value, "unit": "s", "cores": last["cores"], "kind": last["kind"],
+                         "sample": last["sample"]},
+        "e2e": {"value": value, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    del np
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--precision", choices=["half", "single", "double"], default="half")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        print("note: --warmup below 3 raised to 3", file=sys.stderr)
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

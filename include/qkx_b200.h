@@ -204,7 +204,7 @@ typedef struct qkx_solver_params {
   double tol;              /* target for the true residual ||b - M x|| / ||b|| */
   int maxIter;             /* total iteration cap */
   double reliable_delta;   /* FP64 residual recomputation when |r| drops by this factor;
-                              <= 0 picks the default of the sloppy precision (0.1 half, 1e-3 single) */
+                              <= 0 picks the default of the sloppy precision (1e-2 half, 1e-5 single) */
   int use_graphs;          /* replay the inner iteration from a CUDA graph */
   const double* mu;        /* NULL, or nrhs twisted masses (one per right-hand side, the
                               multi-mass solve of CG_EO_MIXED); NULL = the context's mu */
@@ -220,6 +220,14 @@ QKX_API int qkx_invert(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, cons
 /* The same on device fields in the even-odd layout. */
 QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, const double* const* b_dev,
                    double* const* x_dev, qkx_solve_info* info);
+
+/* Autotune the inner hop of CG_EO_MIXED for this lattice, precision and batch
+ * size: times every tile (right-hand sides per thread x threads per block) on
+ * the device and keeps the fastest for later solves (a solve with an untuned
+ * (precision, nrhs) tunes itself first, outside its timed region).  No
+ * reference counterpart. */
+QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread, int* threads_per_block,
+                     double* ms_per_hop);
 
 /* ---------------------------------------------------------------- memory helpers */
 /* Page-locked host memory for fast transfers (cudaHostAlloc); NULL on failure. */
@@ -238,6 +246,9 @@ QKX_API int qkx_memcpy_d2h(qkx_ctx* ctx, void* dst, const void* src, size_t byte
 QKX_API int qkx_profile_enable(qkx_ctx* ctx, int on);
 QKX_API int qkx_profile_read(qkx_ctx* ctx, long long* launches, double* ms, double* bytes);
 QKX_API int qkx_profile_reset(qkx_ctx* ctx);
+/* Kernels this context has launched since creation (a replayed CUDA graph
+ * counts each of its kernel nodes); -1 for a NULL context. */
+QKX_API long long qkx_kernel_launches(const qkx_ctx* ctx);
 
 #ifdef __cplusplus
 }

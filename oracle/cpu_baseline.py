@@ -1,0 +1,120 @@
+"""Timed CPU baseline of the hot path: the reference's own CG (oracle/_ref,
+compiled from the reference sources) or, where that build is absent, the
+oracle's C restatement, run on the host cores.
+
+TEST/BASELINE INFRASTRUCTURE ONLY: used by the CPU-baseline leg and the
+reference arm of bench.py, never by the product path.
+
+The reference is single-threaded (its only parallelism is MPI ranks), so the
+host cores are used the way the reference would use them for a multi-source
+job: one independent single-rank process per source.  A bounded sample --
+`n_iter` CG iterations in each of P concurrent processes on the full lattice --
+gives the time per CG iteration under full-socket load; the projection to the
+whole job is  ceil(n_sources / P) * iterations_to_converge * t_iteration.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+from oracle import oracle as O
+
+
+def _worker(args):
+    kind, L, kappa, mu, links_path, spin, colour, n_iter = args
+    L = tuple(L)
+    V = O.volume(L)
+    U = np.fromfile(links_path, dtype=np.float64).reshape(V, 4, 3, 3, 2)
+    b = O.spinor_point(L, (0, 0, 0, 0), spin, colour)
+    x = np.zeros_like(b)
+    if kind == "reference":
+        lib = O.ref()
+        lib.ref_cg_timed.restype = C.c_double
+        lib.ref_cg_timed.argtypes = [O._ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                     O._dp, O._dp, O._dp]
+        return lib.ref_cg_timed(O._L(L), kappa, mu, 1, 1e-30, n_iter, O._ptr(U), O._ptr(b), O._ptr(x))
+    t0 = time.perf_counter()
+    O.cg(L, U, b, kappa, mu, 1, tol=1e-30, maxIter=n_iter)
+    return time.perf_counter() - t0
+
+
+def iterations_to_converge(L, kappa, mu, eps, seed, tol=1e-10) -> int:
+    """Iterations the reference's CG (its own stopping rule) needs on a lattice
+    small enough to solve quickly, same parameters, point source."""
+    U = O.apply_bc(L, O.gauge_random(L, eps, seed), -1)
+    b = O.spinor_point(L, (0, 0, 0, 0), 0, 0)
+    Mdb = O.apply("tm_dag", L, U, b, kappa, mu, 1)
+    _, k, _ = O.cg(L, U, Mdb, kappa, mu, 1, tol=tol, maxIter=5000)
+    return k
+
+
+def run(L, kappa, mu, eps, seed, n_sources=12, n_iter=1, procs=None, iters_full=None,
+        links: np.ndarray | None = None, timeout: float = 900.0) -> dict:
+    """Time the CPU hot path and project it to solving n_sources point sources.
+
+    Returns {"value": seconds for the whole job, "per_iter_s", "cores", "kind",
+    "sample", "iters_full"}."""
+    O.build(ref=True)
+    kind = "reference" if O.ref_available() else "port"
+    ncpu = os.cpu_count() or 1
+    P = max(1, min(n_sources, ncpu if procs is None else procs))
+    if links is None:
+        links = O.apply_bc(L, O.gauge_random(L, eps, seed), -1)
+    import shutil
+    tmpdir = tempfile.gettempdir()
+    if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > 2 * links.nbytes:
+        tmpdir = "/dev/shm"
+    fd, path = tempfile.mkstemp(prefix="qkx_links_", suffix=".f64", dir=tmpdir)
+    os.close(fd)
+    try:
+        links.astype(np.float64).tofile(path)
+        root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+        env = dict(os.environ, PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
+        t0 = time.perf_counter()
+        procs_ = []
+        for i in range(P):
+            job = [kind, list(L), kappa, mu, path, (i // 3) % 4, i % 3, n_iter]
+            procs_.append(subprocess.Popen([sys.executable, "-m", "oracle.cpu_baseline", json.dumps(job)],
+                                           cwd=root, env=env, stdout=subprocess.PIPE, text=True))
+        times = []
+        deadline = time.time() + timeout
+        for p in procs_:
+            try:
+                out, _ = p.communicate(timeout=max(1.0, deadline - time.time()))
+            except subprocess.TimeoutExpired:
+                for q in procs_:
+                    q.kill()
+                raise RuntimeError("CPU baseline worker timed out")
+            if p.returncode != 0:
+                raise RuntimeError(f"CPU baseline worker failed (rc={p.returncode})")
+            times.append(float(out.strip().splitlines()[-1]))
+        wall = time.perf_counter() - t0
+    finally:
+        os.unlink(path)
+    per_iter = float(np.median(times)) / n_iter
+    if iters_full is None:
+        small = (8, 8, 8, 16)
+        iters_full = iterations_to_converge(small, kappa, mu, eps, seed)
+        src = f"iterations from a full reference-rule solve on {small[0]}^3x{small[3]}"
+    else:
+        src = "iterations from the reference-rule CG replica at full size"
+    value = math.ceil(n_sources / P) * iters_full * per_iter
+    sample = (f"{P} concurrent single-rank {kind} CG processes x {n_iter} iteration(s) on "
+              f"{L[0]}x{L[1]}x{L[2]}x{L[3]} (median {per_iter:.2f} s/iteration under full load, "
+              f"wall {wall:.1f} s); projected to {n_sources} sources x {iters_full} iterations "
+              f"({src})")
+    return {"value": value, "per_iter_s": per_iter, "cores": P, "kind": kind, "sample": sample,
+            "iters_full": iters_full}
+
+
+if __name__ == "__main__":
+    # worker process: time n_iter CG iterations and print the seconds
+    print(_worker(json.loads(sys.argv[1])), flush=True)

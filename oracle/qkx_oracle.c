@@ -9,11 +9,14 @@
  */
 #include "qkx_oracle.h"
 
+#define _POSIX_C_SOURCE 200809L
 #include <complex.h>
 #include <math.h>
+#include <pthread.h>
 #include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
+#include <unistd.h>
 
 typedef double _Complex cplx;
 
@@ -449,9 +452,9 @@ static void reunitarize(cplx* u) {
 
 /* U_mu(x) = exp(i eps H), H = (A + A^+)/2 minus its trace/3, A entries unit
  * complex Gaussians (E|A_ab|^2 = 1: real and imaginary parts N(0, 1/2)). */
-void orc_gauge_random(const int L[4], double eps, unsigned long long seed, double* U) {
-  long V = orc_volume(L);
-  for (long s = 0; s < V; s++)
+static void gauge_random_range(const int L[4], double eps, unsigned long long seed, double* U, long s0,
+                               long s1) {
+  for (long s = s0; s < s1; s++)
     for (int mu = 0; mu < 4; mu++) {
       cplx A[9], X[9];
       for (int k = 0; k < 9; k++) {
@@ -471,6 +474,52 @@ void orc_gauge_random(const int L[4], double eps, unsigned long long seed, doubl
     }
 }
 
+/* the generators split the sites over host threads (the result does not
+ * depend on the split: every entry is a pure function of its counter) */
+typedef struct {
+  const int* L;
+  double eps;
+  unsigned long long seed;
+  double* out;
+  long s0, s1;
+  int kind;
+} gen_job;
+
+static void spinor_gaussian_range(const int L[4], unsigned long long seed, double* psi, long s0, long s1);
+
+static void* gen_worker(void* arg) {
+  gen_job* j = (gen_job*)arg;
+  if (j->kind == 0)
+    gauge_random_range(j->L, j->eps, j->seed, j->out, j->s0, j->s1);
+  else
+    spinor_gaussian_range(j->L, j->seed, j->out, j->s0, j->s1);
+  return NULL;
+}
+
+static void gen_parallel(const int L[4], double eps, unsigned long long seed, double* out, int kind) {
+  long V = orc_volume(L);
+  long nt = sysconf(_SC_NPROCESSORS_ONLN);
+  if (nt < 1) nt = 1;
+  if (nt > 64) nt = 64;
+  if (V < 4096) nt = 1;
+  pthread_t th[64];
+  gen_job jobs[64];
+  for (long t = 0; t < nt; t++) {
+    jobs[t] = (gen_job){L, eps, seed, out, V * t / nt, V * (t + 1) / nt, kind};
+    if (nt == 1) {
+      gen_worker(&jobs[t]);
+    } else {
+      pthread_create(&th[t], NULL, gen_worker, &jobs[t]);
+    }
+  }
+  if (nt > 1)
+    for (long t = 0; t < nt; t++) pthread_join(th[t], NULL);
+}
+
+void orc_gauge_random(const int L[4], double eps, unsigned long long seed, double* U) {
+  gen_parallel(L, eps, seed, U, 0);
+}
+
 void orc_gauge_unit(const int L[4], double* U) {
   long V = orc_volume(L);
   memset(U, 0, sizeof(double) * 72 * V);
@@ -480,8 +529,12 @@ void orc_gauge_unit(const int L[4], double* U) {
 }
 
 void orc_spinor_gaussian(const int L[4], unsigned long long seed, double* psi) {
-  long V = orc_volume(L);
-  for (long s = 0; s < V; s++)
+  gen_parallel(L, 0.0, seed, psi, 1);
+}
+
+static void spinor_gaussian_range(const int L[4], unsigned long long seed, double* psi, long s0, long s1) {
+  (void)L;
+  for (long s = s0; s < s1; s++)
     for (int k = 0; k < 12; k++) {
       double g0, g1;
       normal_pair(seed, STREAM_SPINOR, (uint64_t)s * 12 + k, &g0, &g1);

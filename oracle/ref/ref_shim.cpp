@@ -183,9 +183,7 @@ double ref_blas(int which, const int L[4], double a, double* x, const double* y)
 
 /* CG::operator()(out, in) with the links as given (the caller applies the
  * boundary condition beforehand, as bin/test_invert.cpp:106 does).  x is both
- * the initial content of `out` and the result.  When max_iter_run > 0 the
- * solver runs with maxIter = max_iter_run regardless of tol (used to time a
- * bounded number of iterations). */
+ * the initial content of `out` and the result. */
 void ref_cg(const int L[4], double kappa, double mu, int twistSign, double tol, int maxIter,
             const double* U, const double* in, double* x) {
   LatticeInfo li = make_info(L, kappa, mu, twistSign, -1, tol, maxIter);
@@ -201,6 +199,30 @@ void ref_cg(const int L[4], double kappa, double mu, int twistSign, double tol, 
     cg(vout, vin, &li);
   }
   store_vec(vout, x);
+}
+
+/* CG::operator() as above, returning the wall seconds of the solver call
+ * alone (set-up and copies excluded).  Used for the timed CPU baseline with
+ * maxIter set to a bounded number of iterations. */
+double ref_cg_timed(const int L[4], double kappa, double mu, int twistSign, double tol, int maxIter,
+                    const double* U, const double* in, double* x) {
+  LatticeInfo li = make_info(L, kappa, mu, twistSign, -1, tol, maxIter);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  u.constGauge = true;
+  Vector vin(&li), vout(&li);
+  load_vec(vin, in);
+  load_vec(vout, x);
+  double t0, t1;
+  {
+    QuietStdout q;
+    CG cg(&li, u);
+    t0 = MPI_Wtime();
+    cg(vout, vin, &li);
+    t1 = MPI_Wtime();
+  }
+  store_vec(vout, x);
+  return t1 - t0;
 }
 
 }  // extern "C"

@@ -62,7 +62,7 @@ SYMBOLS = [
     "qkx_cg", "qkx_cg_dev", "qkx_invert", "qkx_invert_dev",
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
-    "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset",
+    "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
 ]
 
 
@@ -149,6 +149,9 @@ def lib() -> C.CDLL:
         L.qkx_profile_enable.argtypes = [_vp, C.c_int]
         L.qkx_profile_read.argtypes = [_vp, C.POINTER(C.c_longlong), _dp, _dp]
         L.qkx_profile_reset.argtypes = [_vp]
+        L.qkx_kernel_launches.argtypes = [_vp]
+        L.qkx_kernel_launches.restype = C.c_longlong
+        L.qkx_tune.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
         _lib = L
     return _lib
 
@@ -341,10 +344,17 @@ class Lattice:
 
     def invert(self, bs: Sequence[np.ndarray], method: int = SOLVER_CG_EO_MIXED,
                precision: int = PREC_HALF, tol: float = 1e-10, maxIter: int = 10000,
-               reliable_delta: float = 0.0, use_graphs: int = 1, strict: bool = True):
-        """Solve M x_i = b_i to ||b - M x|| / ||b|| <= tol (FP64 true residual)."""
+               reliable_delta: float = 0.0, use_graphs: int = 1, strict: bool = True,
+               out: Sequence[np.ndarray] | None = None):
+        """Solve M x_i = b_i to ||b - M x|| / ||b|| <= tol (FP64 true residual).
+        `out` may supply the solution arrays (e.g. page-locked buffers)."""
         bs = [_host(b) for b in bs]
-        xs = [np.empty((self.V, 4, 3, 2)) for _ in bs]
+        if out is not None:
+            xs = list(out)
+            for x in xs:
+                assert x.dtype == np.float64 and x.flags["C_CONTIGUOUS"] and x.size == self.V * 24
+        else:
+            xs = [np.empty((self.V, 4, 3, 2)) for _ in bs]
         n = len(bs)
         bp = (_vp * n)(*[b.ctypes.data for b in bs])
         xp = (_vp * n)(*[x.ctypes.data for x in xs])
@@ -381,6 +391,31 @@ class Lattice:
 
     def sync(self) -> None:
         check(lib().qkx_sync(self.ctx))
+
+    def tune(self, precision: int = PREC_HALF, nrhs: int = 12):
+        """Autotune the inner hop; returns (rhs_per_thread, threads_per_block, ms_per_hop)."""
+        nr, nt, ms = C.c_int(), C.c_int(), C.c_double()
+        check(lib().qkx_tune(self.ctx, precision, nrhs, C.byref(nr), C.byref(nt), C.byref(ms)))
+        return nr.value, nt.value, ms.value
+
+    def kernel_launches(self) -> int:
+        return int(lib().qkx_kernel_launches(self.ctx))
+
+    def stream(self) -> int:
+        return int(lib().qkx_stream(self.ctx) or 0)
+
+
+def pinned_array(shape) -> np.ndarray:
+    """A float64 numpy array in page-locked host memory (freed with the array)."""
+    n = int(np.prod(shape))
+    ptr = lib().qkx_host_alloc(n * 8)
+    if not ptr:
+        raise QkxError(ERR_NOMEM, "page-locked host allocation failed")
+    buf = (C.c_double * n).from_address(ptr)
+    arr = np.ctypeslib.as_array(buf).reshape(shape)
+    import weakref
+    weakref.finalize(buf, lib().qkx_host_free, ptr)
+    return arr
 
 
 def check_nonneg(rc: int) -> int:

@@ -8,6 +8,7 @@
 
 #include "blas.cuh"
 #include "hop.cuh"
+#include "hop_c3.cuh"
 #include "layout.cuh"
 #include "qkx_ctx.cuh"
 #include "site_ops.cuh"
@@ -70,9 +71,36 @@ int prof_collect(qkx_ctx* c) {
   return QKX_OK;
 }
 
+// ---------------------------------------------------------------- lazy buffers
+// The host-layout staging buffer and the FP64 work fields are allocated when a
+// call first needs them, so a context that only tunes or runs the batched
+// solver on device fields does not hold them.
+int ensure_stage(qkx_ctx* c) {
+  if (c->stage) return QKX_OK;
+  cudaError_t e = cudaMalloc(&c->stage, sizeof(double2) * 12 * c->V);
+  if (e != cudaSuccess) {
+    set_error("staging buffer: %s", cudaGetErrorString(e));
+    return QKX_ERR_NOMEM;
+  }
+  return QKX_OK;
+}
+
+int ensure_work(qkx_ctx* c) {
+  for (int i = 0; i < qkx_ctx::NW; i++) {
+    if (c->w[i]) continue;
+    cudaError_t e = cudaMalloc(&c->w[i], sizeof(double2) * 12 * c->V);
+    if (e != cudaSuccess) {
+      set_error("work field: %s", cudaGetErrorString(e));
+      return QKX_ERR_NOMEM;
+    }
+  }
+  return QKX_OK;
+}
+
 // ---------------------------------------------------------------- reductions
 int finalize(qkx_ctx* c, int nparts, int mode, double* dst, int rhs) {
   k_finalize<<<1, 1024, 0, c->st>>>(c->part, nparts, dst, mode, c->sc, rhs);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
 }
@@ -80,6 +108,7 @@ int finalize(qkx_ctx* c, int nparts, int mode, double* dst, int rhs) {
 int redot(qkx_ctx* c, const double2* x, const double2* y, size_t n, int mode, double* dst, int rhs) {
   int g = blas_grid(n);
   k_redot<<<g, BLAS_NT, 0, c->st>>>(x, y, n, c->part);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   return finalize(c, g, mode, dst, rhs);
 }
@@ -92,6 +121,9 @@ int redot(qkx_ctx* c, const double2* x, const double2* y, size_t n, int mode, do
 static double hop_bytes(size_t nout, double S, double G, bool both, bool extra_x) {
   return (double)nout * (2 * S + (both ? 4 : 8) * G + (extra_x ? S : 0));
 }
+
+// FP64 sites per block of the colour-split kernel (x 3 colour threads)
+constexpr int C3_NS = 64;
 
 template <int B, bool DAG, int EPI>
 static int hop64_t(qkx_ctx* c, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_distinct, int out_parity,
@@ -108,16 +140,68 @@ static int hop64_t(qkx_ctx* c, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_
   A.s = s;
   A.norm_part = norm_part;
   A.nrhs = 1;
-  A.nblk = hop_blocks_per_rhs<128>(c->Vh, out_parity);
+  A.nblk = c3_blocks_per_rhs<C3_NS>(c->Vh, out_parity);
   A.cvec = nullptr;
   A.svec = nullptr;
   A.active = nullptr;
   const int n = out_parity < 0 ? 2 * c->Vh : c->Vh;
   QKX_TRY(prof_begin(c));
-  hop_kernel<128, SpinorF64, GaugeF64x18, double, B, DAG, EPI><<<A.nblk, 128, 0, c->st>>>(A);
+  hop_c3_kernel<C3_NS, SpinorF64, B, DAG, EPI><<<A.nblk, dim3(C3_NS, 3), 0, c->st>>>(A);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   bool extra = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV) && x_distinct;
   return prof_end(c, hop_bytes(n, 192.0, 144.0, out_parity < 0, extra));
+}
+
+// Batched FP64 hop (UKQCD basis, D not D^+) over nrhs right-hand sides stored
+// [rhs][12][Vh] per parity, per-RHS twist factors and mask; returns the
+// number of norm partials per RHS in *nblk.
+template <int EPI>
+static int hop64_batch_t(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 out, SpinorF64 x, int out_parity, double a,
+                         double csign, const double* cvec, const double* svec, const int* active, double* norm_part,
+                         int* nblk) {
+  HopArgs<SpinorF64, GaugeF64x18> A;
+  A.out = out;
+  A.in = in;
+  A.x = x;
+  A.gauge = GaugeF64x18{c->U18, c->Vh};
+  A.g = c->geom;
+  A.out_parity = out_parity;
+  A.a = a;
+  A.c = csign;
+  A.s = 1.0;
+  A.norm_part = norm_part;
+  A.nrhs = nrhs;
+  A.nblk = c3_blocks_per_rhs<C3_NS>(c->Vh, out_parity);
+  A.cvec = cvec;
+  A.svec = svec;
+  A.active = active;
+  hop_c3_kernel<C3_NS, SpinorF64, 0, false, EPI><<<A.nblk * nrhs, dim3(C3_NS, 3), 0, c->st>>>(A);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  if (nblk) *nblk = A.nblk;
+  return QKX_OK;
+}
+
+int hop64_batch(qkx_ctx* c, int epi, int nrhs, SpinorF64 in, SpinorF64 out, SpinorF64 x, int out_parity, double a,
+                double csign, const double* cvec, const double* svec, const int* active, double* norm_part,
+                int* nblk) {
+  switch (epi) {
+    case EPI_PLAIN:
+      return hop64_batch_t<EPI_PLAIN>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active, norm_part, nblk);
+    case EPI_XPAY:
+      return hop64_batch_t<EPI_XPAY>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active, norm_part, nblk);
+    case EPI_XPAY_G5:
+      return hop64_batch_t<EPI_XPAY_G5>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active, norm_part,
+                                        nblk);
+    case EPI_TWIST_INV:
+      return hop64_batch_t<EPI_TWIST_INV>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active, norm_part,
+                                          nblk);
+    case EPI_XPAY_TWINV:
+      return hop64_batch_t<EPI_XPAY_TWINV>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active,
+                                           norm_part, nblk);
+  }
+  return invalid("epilogue");
 }
 
 // runtime -> compile-time dispatch, on accessors (single-parity fields allowed)
@@ -150,9 +234,15 @@ int site_op_acc(qkx_ctx* c, int basis, int op, SpinorF64 in, SpinorF64 out, int 
   const int n = npar * c->Vh;
   const int nb = (n + 255) / 256;
   if (basis == 0)
-    k_site_op<0><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
+    {
+      k_site_op<0><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
+      counted(c);
+    }
   else
-    k_site_op<1><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
+    {
+      k_site_op<1><<<nb, 256, 0, c->st>>>(in, out, par_first, npar, op, cc, s);
+      counted(c);
+    }
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
 }
@@ -189,6 +279,7 @@ static int tm_xx(qkx_ctx* c, int basis, int par, double sgn, const double2* in, 
 }
 
 int run_op(qkx_ctx* c, int op, const double2* in, double2* out) {
+  QKX_TRY(ensure_work(c));
   if (!c->have_gauge && op != QKX_OP_GAMMA5 && op != QKX_OP_GAMMA5_CHIRAL && op != QKX_OP_TWIST &&
       op != QKX_OP_TWIST_INV && op != QKX_OP_TWIST_DAG && op != QKX_OP_TWIST_DAG_INV &&
       op != QKX_OP_TWIST_INV_CHIRAL && op != QKX_OP_ROTATE_CHIRAL_TO_UKQCD) {
@@ -258,14 +349,18 @@ int run_op(qkx_ctx* c, int op, const double2* in, double2* out) {
 }
 
 static int upload_spinor(qkx_ctx* c, const double* host, double2* dev) {
+  QKX_TRY(ensure_stage(c));
   QKX_CUDA(cudaMemcpyAsync(c->stage, host, sizeof(double2) * 12 * c->V, cudaMemcpyHostToDevice, c->st));
   k_spinor_aos_to_eo<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->stage, dev, c->geom);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
 }
 
 static int download_spinor(qkx_ctx* c, const double2* dev, double* host) {
+  QKX_TRY(ensure_stage(c));
   k_spinor_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(dev, c->stage, c->geom);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   QKX_CUDA(cudaMemcpyAsync(host, c->stage, sizeof(double2) * 12 * c->V, cudaMemcpyDeviceToHost, c->st));
   return QKX_OK;
@@ -281,6 +376,7 @@ static int gauge_finish(qkx_ctx* c) {
   double* part = nullptr;
   QKX_CUDA(cudaMallocAsync(&part, sizeof(double) * 4 * nb, c->st));
   k_gauge_check<<<nb, 256, 0, c->st>>>(c->U18, c->geom, part);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   std::vector<double> h((size_t)4 * nb);
   QKX_CUDA(cudaMemcpyAsync(h.data(), part, sizeof(double) * 4 * nb, cudaMemcpyDeviceToHost, c->st));
@@ -305,10 +401,11 @@ static int gauge_finish(qkx_ctx* c) {
       QKX_CUDA(cudaMalloc(&c->U12hb, sizeof(uint2) * 8 * (size_t)c->Vh));
     }
     k_gauge_compress<<<nb, 256, 0, c->st>>>(c->U18, c->geom, c->raw_sign, nullptr, c->U12f, c->U12ha, c->U12hb);
+    counted(c);
     QKX_CUDA(cudaGetLastError());
   }
   c->have_gauge = 1;
-  if (c->mixed) mixed_free(c);
+  mixed_invalidate(c);
   return QKX_OK;
 }
 
@@ -359,10 +456,8 @@ int qkx_create(const qkx_params* p, int device, qkx_ctx** out) {
   if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) != cudaSuccess) fail(e, "stream");
   const size_t fbytes = sizeof(double2) * 12 * c->V;
   if (rc == QKX_OK && (e = cudaMalloc(&c->U18, sizeof(double2) * 36 * c->V)) != cudaSuccess) fail(e, "links");
-  if (rc == QKX_OK && (e = cudaMalloc(&c->stage, fbytes)) != cudaSuccess) fail(e, "staging");
-  for (int i = 0; i < qkx_ctx::NW && rc == QKX_OK; i++)
-    if ((e = cudaMalloc(&c->w[i], fbytes)) != cudaSuccess) fail(e, "work field");
-  c->npart = std::max(148 * 8, (int)((2 * (size_t)c->Vh + 127) / 128)) + 1;
+  (void)fbytes;  // the staging buffer and the FP64 work fields are allocated on first use
+  c->npart = std::max(148 * 8, 2 * (int)((c->Vh + 31) / 32)) + 1;  // room for any hop block size >= 32
   if (rc == QKX_OK && (e = cudaMalloc(&c->part, sizeof(double) * c->npart)) != cudaSuccess) fail(e, "partials");
   if (rc == QKX_OK && (e = cudaMalloc(&c->sc, sizeof(CgScalars))) != cudaSuccess) fail(e, "scalars");
   if (rc == QKX_OK && (e = cudaHostAlloc(&c->sc_h, sizeof(CgScalars), cudaHostAllocDefault)) != cudaSuccess)
@@ -442,6 +537,7 @@ int qkx_load_gauge(qkx_ctx* c, const double* U_host, int bc_mode) {
   QKX_CUDA(cudaMemcpyAsync(tmp, U_host, bytes, cudaMemcpyHostToDevice, c->st));
   int tsign = (bc_mode == QKX_LINKS_APPLY_BC && c->p.boundaryT == -1) ? -1 : 1;
   k_gauge_aos_to_eo<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(tmp, c->U18, c->geom, tsign);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   QKX_CUDA(cudaFreeAsync(tmp, c->st));
   return gauge_finish(c);
@@ -453,6 +549,7 @@ int qkx_gauge_generate(qkx_ctx* c, double eps, unsigned long long seed, int bc_m
   QKX_CUDA(cudaSetDevice(c->device));
   const int nl = 8 * c->Vh;
   k_gauge_generate<<<(nl + 127) / 128, 128, 0, c->st>>>(c->U18, c->geom, eps, seed);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   if (bc_mode == QKX_LINKS_APPLY_BC && c->p.boundaryT == -1) {
     // multiply the last slice's t-links by -1 in place (the aos->eo kernel
@@ -461,7 +558,9 @@ int qkx_gauge_generate(qkx_ctx* c, double eps, unsigned long long seed, int bc_m
     const size_t bytes = sizeof(double2) * 36 * c->V;
     QKX_CUDA(cudaMallocAsync(&tmp, bytes, c->st));
     k_gauge_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->U18, tmp, c->geom);
+    counted(c);
     k_gauge_aos_to_eo<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(tmp, c->U18, c->geom, -1);
+    counted(c);
     QKX_CUDA(cudaGetLastError());
     QKX_CUDA(cudaFreeAsync(tmp, c->st));
   }
@@ -479,6 +578,7 @@ int qkx_download_gauge(qkx_ctx* c, double* U_host) {
   const size_t bytes = sizeof(double2) * 36 * c->V;
   QKX_CUDA(cudaMallocAsync(&tmp, bytes, c->st));
   k_gauge_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->U18, tmp, c->geom);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   QKX_CUDA(cudaMemcpyAsync(U_host, tmp, bytes, cudaMemcpyDeviceToHost, c->st));
   QKX_CUDA(cudaFreeAsync(tmp, c->st));
@@ -503,6 +603,7 @@ int qkx_apply(qkx_ctx* c, int op, const double* in_host, double* out_host) {
   if (!c || !in_host || !out_host) return invalid("NULL argument");
   if (op < 0 || op >= QKX_OP_COUNT) return invalid("operator id");
   QKX_CUDA(cudaSetDevice(c->device));
+  QKX_TRY(ensure_work(c));
   QKX_TRY(upload_spinor(c, in_host, c->w[0]));
   QKX_TRY(run_op(c, op, c->w[0], c->w[1]));
   QKX_TRY(download_spinor(c, c->w[1], out_host));
@@ -542,6 +643,7 @@ int qkx_X_eq_X_p_aY(qkx_ctx* c, double* x, double a, const double* y) {
   QKX_CUDA(cudaSetDevice(c->device));
   size_t n = 12 * c->V;
   k_axpy_h<<<blas_grid(n), BLAS_NT, 0, c->st>>>(a, (const double2*)y, (double2*)x, n);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
 }
@@ -551,6 +653,7 @@ int qkx_X_eq_aX_p_Y(qkx_ctx* c, double* x, double a, const double* y) {
   QKX_CUDA(cudaSetDevice(c->device));
   size_t n = 12 * c->V;
   k_xpay_h<<<blas_grid(n), BLAS_NT, 0, c->st>>>((const double2*)y, a, (double2*)x, n);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
 }
@@ -567,11 +670,14 @@ static int cg_fp64_loop(qkx_ctx* c, double2* x, double2* r, double2* p, double2*
     QKX_TRY(apply_tm(c, p, tmp, false));                     // Ap.tmDagtm(p, tmp, ...)
     QKX_TRY(apply_tm(c, tmp, Ap, true));
     QKX_TRY(redot(c, p, Ap, n, FIN_PAP, nullptr, 0));         // pAp, alpha = r2 / pAp
-    k_axpy<<<g, BLAS_NT, 0, c->st>>>(c->sc->alpha, 1.0, p, x, n);    // x = x + alpha p
-    k_axpy<<<g, BLAS_NT, 0, c->st>>>(c->sc->alpha, -1.0, Ap, r, n);  // r = r - alpha Ap
+    k_axpy<<<g, BLAS_NT, 0, c->st>>>(c->sc->alpha, 1.0, p, x, n);
+    counted(c);    // x = x + alpha p
+    k_axpy<<<g, BLAS_NT, 0, c->st>>>(c->sc->alpha, -1.0, Ap, r, n);
+    counted(c);  // r = r - alpha Ap
     QKX_CUDA(cudaGetLastError());
     QKX_TRY(redot(c, r, r, n, FIN_R2, nullptr, 0));           // r2, beta = r2 / r2_old
-    k_xpay<<<g, BLAS_NT, 0, c->st>>>(r, c->sc->beta, p, n);          // p = r + beta p
+    k_xpay<<<g, BLAS_NT, 0, c->st>>>(r, c->sc->beta, p, n);
+    counted(c);          // p = r + beta p
     QKX_CUDA(cudaGetLastError());
     (*k)++;
     QKX_CUDA(cudaMemcpyAsync(c->hscal, c->sc->r2, sizeof(double), cudaMemcpyDeviceToHost, c->st));
@@ -608,6 +714,7 @@ int qkx_cg_dev(qkx_ctx* c, const double* in_dev, double* x_dev, qkx_solve_info* 
     return QKX_ERR_NOGAUGE;
   }
   QKX_CUDA(cudaSetDevice(c->device));
+  QKX_TRY(ensure_work(c));
   double2 *r = c->w[2], *p = c->w[3], *Ap = c->w[4], *tmp = c->w[5];
   const double2* in = (const double2*)in_dev;
   double2* x = (double2*)x_dev;
@@ -642,6 +749,7 @@ int qkx_cg_dev(qkx_ctx* c, const double* in_dev, double* x_dev, qkx_solve_info* 
 int qkx_cg(qkx_ctx* c, const double* in_host, double* x_host, qkx_solve_info* info) {
   if (!c || !in_host || !x_host) return invalid("NULL argument");
   QKX_CUDA(cudaSetDevice(c->device));
+  QKX_TRY(ensure_work(c));
   QKX_TRY(upload_spinor(c, in_host, c->w[0]));
   QKX_TRY(upload_spinor(c, x_host, c->w[1]));
   int rc = qkx_cg_dev(c, (const double*)c->w[0], (double*)c->w[1], info);
@@ -658,6 +766,7 @@ static int true_residual(qkx_ctx* c, const double2* b, const double2* x, double*
   QKX_TRY(apply_tm(c, x, c->w[6], false));
   int g = blas_grid(n);
   k_sub_norm<<<g, BLAS_NT, 0, c->st>>>(b, c->w[6], c->w[6], n, c->part);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   QKX_TRY(finalize(c, g, FIN_STORE, c->dscal + 2, 0));
   QKX_TRY(redot(c, b, b, n, FIN_STORE, c->dscal + 3, 0));
@@ -672,6 +781,7 @@ static int true_residual(qkx_ctx* c, const double2* b, const double2* x, double*
 // continues with a proportionally tighter stop.
 static int invert_cg_fp64(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
                           double2* const* x, qkx_solve_info* info) {
+  QKX_TRY(ensure_work(c));
   double2 *in = c->w[0], *r = c->w[2], *p = c->w[3], *Ap = c->w[4], *tmp = c->w[5];
   const size_t n = 12 * c->V;
   for (int i = 0; i < nrhs; i++) {
@@ -828,6 +938,20 @@ int qkx_profile_read(qkx_ctx* c, long long* launches, double* ms, double* bytes)
   if (bytes) *bytes = c->prof_bytes;
   return QKX_OK;
 }
+long long qkx_kernel_launches(const qkx_ctx* c) { return c ? c->kernels : -1; }
+
+int qkx_tune(qkx_ctx* c, int precision, int nrhs, int* rhs_per_thread, int* threads_per_block,
+             double* ms_per_hop) {
+  if (!c) return invalid("ctx is NULL");
+  if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
+  if (!c->have_gauge) {
+    set_error("tuning needs a gauge field");
+    return QKX_ERR_NOGAUGE;
+  }
+  QKX_CUDA(cudaSetDevice(c->device));
+  return tune(c, precision, nrhs, rhs_per_thread, threads_per_block, ms_per_hop);
+}
+
 int qkx_profile_reset(qkx_ctx* c) {
   if (!c) return invalid("ctx is NULL");
   QKX_TRY(prof_collect(c));

@@ -33,6 +33,7 @@
 
 #include "blas.cuh"
 #include "hop.cuh"
+#include "hop_mrhs.cuh"
 #include "qkx_ctx.cuh"
 #include "site_ops.cuh"
 
@@ -45,7 +46,7 @@ struct PHalf {
   using GA = GaugeF16x12;
   using R = float;
   using AC = SpinorF32;
-  static constexpr double S = 52.0, G = 24.0, delta = 0.1;
+  static constexpr double S = 52.0, G = 24.0, delta = 1e-2;
 };
 struct PSingle {
   static constexpr int id = QKX_PREC_SINGLE;
@@ -53,7 +54,7 @@ struct PSingle {
   using GA = GaugeF32x12;
   using R = float;
   using AC = SpinorF32;
-  static constexpr double S = 96.0, G = 48.0, delta = 1e-3;
+  static constexpr double S = 96.0, G = 48.0, delta = 1e-5;
 };
 struct PDouble {
   static constexpr int id = QKX_PREC_DOUBLE;
@@ -332,6 +333,8 @@ struct MixedState {
   double* part = nullptr;  // [R][max(nblk, MX_GRID)]
   cudaGraphExec_t graph = nullptr;
   int graph_R = 0;
+  int graph_nr = 0, graph_nt = 0;  // hop tile the graph was captured with
+  long long graph_kernels = 0;    // kernel nodes in the graph
   double graph_kappa = 0;         // kappa^2 is a kernel argument inside the graph
   std::vector<cudaEvent_t> gev;   // event pairs captured around the hop kernels
 };
@@ -351,28 +354,38 @@ void mixed_free(qkx_ctx* c) {
   c->mixed = nullptr;
 }
 
+// Sloppy hop fields (p, Ap, t, y) for R right-hand sides; with `solver` also
+// the accumulators and FP64 batches the solve needs (tuning needs only the former).
 template <class P>
-static int mixed_alloc(qkx_ctx* c, int R) {
-  if (c->mixed && c->mixed->prec == P::id && c->mixed->R >= R) return QKX_OK;
-  mixed_free(c);
-  MixedState* m = new MixedState();
-  c->mixed = m;
-  m->prec = P::id;
-  m->R = R;
+static int mixed_alloc(qkx_ctx* c, int R, bool solver) {
+  MixedState* m = c->mixed;
+  if (m && (m->prec != P::id || m->R < R)) {
+    mixed_free(c);
+    m = nullptr;
+  }
+  if (!m) {
+    m = new MixedState();
+    c->mixed = m;
+    m->prec = P::id;
+    m->R = R;
+  }
   const int Vh = c->Vh;
   int rc = QKX_OK;
   for (BField* f : {&m->p, &m->Ap, &m->t, &m->y})
-    if (rc == QKX_OK) rc = bfield_alloc<typename P::SP>(*f, R, Vh);
-  for (BField* f : {&m->rs, &m->xs})
-    if (rc == QKX_OK) rc = bfield_alloc<typename P::AC>(*f, R, Vh);
-  const size_t h64 = sizeof(double2) * 12 * (size_t)Vh * R;
-  for (double2** f : {&m->bE, &m->bO, &m->x64, &m->g5bh, &m->t64, &m->z64, &m->r64})
-    if (rc == QKX_OK && cudaMalloc(f, h64) != cudaSuccess) rc = QKX_ERR_NOMEM;
-  if (rc == QKX_OK && cudaMalloc(&m->cvec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
-  if (rc == QKX_OK && cudaMalloc(&m->svec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
-  const int nblk = hop_blocks_per_rhs<128>(Vh, -1);
-  if (rc == QKX_OK && cudaMalloc(&m->part, sizeof(double) * (size_t)R * std::max(nblk, MX_GRID)) != cudaSuccess)
+    if (rc == QKX_OK && !f->d) rc = bfield_alloc<typename P::SP>(*f, m->R, Vh);
+  if (rc == QKX_OK && !m->cvec && cudaMalloc(&m->cvec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  if (rc == QKX_OK && !m->svec && cudaMalloc(&m->svec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  // partials: the smallest hop block (64 threads) over both parities, or the streaming grid
+  const size_t nblk = (size_t)hop_blocks_per_rhs<64>(Vh, -1) + MX_GRID;
+  if (rc == QKX_OK && !m->part && cudaMalloc(&m->part, sizeof(double) * (size_t)m->R * nblk) != cudaSuccess)
     rc = QKX_ERR_NOMEM;
+  if (solver) {
+    for (BField* f : {&m->rs, &m->xs})
+      if (rc == QKX_OK && !f->d) rc = bfield_alloc<typename P::AC>(*f, m->R, Vh);
+    const size_t h64 = sizeof(double2) * 12 * (size_t)Vh * m->R;
+    for (double2** f : {&m->bE, &m->bO, &m->x64, &m->g5bh, &m->t64, &m->z64, &m->r64})
+      if (rc == QKX_OK && !*f && cudaMalloc(f, h64) != cudaSuccess) rc = QKX_ERR_NOMEM;
+  }
   if (rc != QKX_OK) {
     mixed_free(c);
     set_error("mixed solver: device allocation for %d right-hand sides failed", R);
@@ -405,11 +418,68 @@ static int hop_batch(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, 
   A.svec = with_s ? m->svec : nullptr;
   A.active = c->sc->active;
   if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
-  hop_kernel<128, SP, GA, R, 0, false, EPI><<<A.nblk * R_, 128, 0, c->st>>>(A);
+  {
+    hop_kernel<128, SP, GA, R, 0, false, EPI><<<A.nblk * R_, 128, 0, c->st>>>(A);
+    counted(c);
+  }
   QKX_CUDA(cudaGetLastError());
   if (prof_slot >= 0)
     QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot + 1], c->st, cudaEventRecordExternal));
   return QKX_OK;
+}
+
+// ---------------------------------------------------------------- multi-RHS sloppy hop
+// Tile of the sloppy hop: NR right-hand sides per thread, NT threads per block.
+struct HopTile {
+  int nr = 0, nt = 0;
+};
+static const HopTile kTiles[] = {{1, 64}, {1, 128}, {1, 256}, {2, 64}, {2, 128}, {2, 256},
+                                 {3, 64}, {3, 128}, {3, 256}, {4, 64}, {4, 128}, {4, 256}};
+
+template <int NT, int NR, class SP, class GA, typename R, int EPI>
+static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x, int out_parity,
+                       double a, double csign, bool with_s, double* norm_part, int prof_slot) {
+  MixedState* m = c->mixed;
+  HopArgs<SP, GA> A;
+  A.out = out;
+  A.in = in;
+  A.x = x;
+  A.gauge = gauge;
+  A.g = g;
+  A.out_parity = out_parity;
+  A.a = a;
+  A.c = csign;
+  A.s = 1.0;
+  A.norm_part = norm_part;
+  A.nrhs = R_;
+  A.nblk = mrhs_site_blocks<NT>(c->Vh);
+  A.cvec = m->cvec;
+  A.svec = with_s ? m->svec : nullptr;
+  A.active = c->sc->active;
+  const int ngrp = (R_ + NR - 1) / NR;
+  if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
+  hop_mrhs_kernel<NT, NR, SP, GA, R, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  if (prof_slot >= 0)
+    QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot + 1], c->st, cudaEventRecordExternal));
+  return QKX_OK;
+}
+
+template <class SP, class GA, typename R, int EPI>
+static int hop_tile(qkx_ctx* c, HopTile t, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x,
+                    int out_parity, double a, double csign, bool with_s, double* norm_part, int prof_slot) {
+#define QKX_TILE(NR_, NT_)                                                                                  \
+  if (t.nr == NR_ && t.nt == NT_)                                                                         \
+    return launch_mrhs<NT_, NR_, SP, GA, R, EPI>(c, R_, gauge, g, in, out, x, out_parity, a, csign, with_s, \
+                                                 norm_part, prof_slot);
+  QKX_TILE(1, 64) QKX_TILE(1, 128) QKX_TILE(1, 256)
+  QKX_TILE(2, 64) QKX_TILE(2, 128) QKX_TILE(2, 256)
+  QKX_TILE(3, 64) QKX_TILE(3, 128) QKX_TILE(3, 256)
+  QKX_TILE(4, 64) QKX_TILE(4, 128) QKX_TILE(4, 256)
+#undef QKX_TILE
+  set_error("invalid hop tile (%d, %d)", t.nr, t.nt);
+  return QKX_ERR_INVALID;
 }
 
 template <class P>
@@ -423,7 +493,7 @@ struct Sloppy {
   static Geom geom(qkx_ctx* c) { return std::is_same<P, PDouble>::value ? c->geom : c->geom_raw; }
 
   // one inner CG iteration for all right-hand sides (graph-capturable)
-  static int iteration(qkx_ctx* c, int R_, bool prof) {
+  static int iteration(qkx_ctx* c, int R_, bool prof, HopTile tile) {
     MixedState* m = c->mixed;
     const int Vh = c->Vh;
     using FT = FieldTraits<SP>;
@@ -431,18 +501,26 @@ struct Sloppy {
     SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh), Ap = FT::acc(m->Ap, 0, Vh);
     AC xs = FA::acc(m->xs, 0, Vh), rs = FA::acc(m->rs, 0, Vh);
     const double k2 = c->p.kappa * c->p.kappa;
-    const int nblk = hop_blocks_per_rhs<128>(Vh, 0);
+    const int nblk = (Vh + tile.nt - 1) / tile.nt;
     const GA U = gauge(c);
     const Geom g = geom(c);
-    QKX_TRY((hop_batch<SP, GA, R, EPI_TWIST_INV>(c, R_, U, g, p, t, p, 1, 0.0, +1.0, true, nullptr, prof ? 0 : -1)));
-    QKX_TRY((hop_batch<SP, GA, R, EPI_XPAY_G5>(c, R_, U, g, t, y, p, 0, -k2, +1.0, false, m->part, prof ? 1 : -1)));
+    QKX_TRY((hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, p, t, p, 1, 0.0, +1.0, true, nullptr,
+                                                prof ? 0 : -1)));
+    QKX_TRY((hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, y, p, 0, -k2, +1.0, false, m->part,
+                                              prof ? 1 : -1)));
     k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, nblk, FIN_PAP, c->sc);
-    QKX_TRY((hop_batch<SP, GA, R, EPI_TWIST_INV>(c, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr, prof ? 2 : -1)));
-    QKX_TRY((hop_batch<SP, GA, R, EPI_XPAY_G5>(c, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr, prof ? 3 : -1)));
+    counted(c);
+    QKX_TRY((hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr,
+                                                prof ? 2 : -1)));
+    QKX_TRY((hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr,
+                                              prof ? 3 : -1)));
     dim3 gr(MX_GRID, R_);
     k_mx_update_xr<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, Ap, xs, rs, c->sc, m->part);
+    counted(c);
     k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, MX_GRID, FIN_R2, c->sc);
+    counted(c);
     k_mx_update_p<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, rs, c->sc);
+    counted(c);
     QKX_CUDA(cudaGetLastError());
     return QKX_OK;
   }
@@ -469,19 +547,87 @@ GaugeF64x18 Sloppy<PDouble>::gauge(qkx_ctx* c) {
   return GaugeF64x18{c->U18, c->Vh};
 }
 
+// ---------------------------------------------------------------- autotuner
+// Times the two inner hop shapes (TWIST_INV then XPAY_G5 with the fused norm)
+// for every tile on this lattice and batch, on the solver's own fields, and
+// keeps the fastest.  The result is cached in the context per (precision,
+// batch size) and survives gauge reloads.
+template <class P>
+static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
+  using SP = typename P::SP;
+  using GA = typename P::GA;
+  using R = typename P::R;
+  using FT = FieldTraits<SP>;
+  MixedState* m = c->mixed;
+  const int Vh = c->Vh;
+  SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh);
+  const GA U = Sloppy<P>::gauge(c);
+  const Geom g = Sloppy<P>::geom(c);
+  CgScalars* sh = c->sc_h;
+  for (int i = 0; i < MAX_RHS; i++) sh->active[i] = i < R_ ? 1 : 0;
+  QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemsetAsync(m->p.d, 0, FT::words * 16 * (size_t)Vh * R_, c->st));
+  if (m->p.n) QKX_CUDA(cudaMemsetAsync(m->p.n, 0, sizeof(float) * (size_t)Vh * R_, c->st));
+  cudaEvent_t e0, e1;
+  QKX_CUDA(cudaEventCreate(&e0));
+  QKX_CUDA(cudaEventCreate(&e1));
+  *best_ms = 1e30;
+  const double k2 = c->p.kappa * c->p.kappa;
+  int rc = QKX_OK;
+  for (const HopTile& tile : kTiles) {
+    if (tile.nr > 1 && tile.nr > R_) continue;
+    for (int rep = 0; rep < 4 && rc == QKX_OK; rep++) {
+      if (rep == 1) rc = cudaEventRecord(e0, c->st) == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+      if (rc == QKX_OK)
+        rc = hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, p, t, p, 1, 0.0, 1.0, true, nullptr, -1);
+      if (rc == QKX_OK)
+        rc = hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, y, p, 0, -k2, 1.0, false, m->part, -1);
+    }
+    if (rc != QKX_OK) break;
+    if (cudaEventRecord(e1, c->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
+      rc = QKX_ERR_CUDA;
+      break;
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e0, e1);
+    const double per_hop = ms / 6.0;
+    if (per_hop < *best_ms) {
+      *best_ms = per_hop;
+      *best = tile;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc == QKX_OK) c->tuned[P::id * 1000 + R_] = {best->nr, best->nt};
+  return rc;
+}
+
+template <class P>
+static int tile_for(qkx_ctx* c, int R_, HopTile* tile) {
+  auto it = c->tuned.find(P::id * 1000 + R_);
+  if (it != c->tuned.end()) {
+    tile->nr = it->second.first;
+    tile->nt = it->second.second;
+    return QKX_OK;
+  }
+  double ms;
+  return tune_tile<P>(c, R_, tile, &ms);
+}
+
 // ---------------------------------------------------------------- batched FP64 pieces
 using H18 = GaugeF64x18;
 
 // out(r) = g5 Mh(csign * c_r) v(r) for the active RHS, through t64; optional |out|^2 partials
-static int schur64_g5_batch(qkx_ctx* c, int R_, double csign, double2* v, double2* out, double* norm_part) {
+// (*nblk of them per RHS)
+static int schur64_g5_batch(qkx_ctx* c, int R_, double csign, double2* v, double2* out, double* norm_part,
+                            int* nblk = nullptr) {
   MixedState* m = c->mixed;
   const int Vh = c->Vh;
   const double k = c->p.kappa;
-  const H18 U{c->U18, Vh};
-  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_TWIST_INV>(c, R_, U, c->geom, B64(v, 0, Vh), B64(m->t64, 1, Vh),
-                                                            B64(v, 0, Vh), 1, 0.0, csign, true, nullptr, -1)));
-  return hop_batch<SpinorF64, H18, double, EPI_XPAY_G5>(c, R_, U, c->geom, B64(m->t64, 1, Vh), B64(out, 0, Vh),
-                                                        B64(v, 0, Vh), 0, -k * k, csign, false, norm_part, -1);
+  QKX_TRY(hop64_batch(c, EPI_TWIST_INV, R_, B64(v, 0, Vh), B64(m->t64, 1, Vh), B64(v, 0, Vh), 1, 0.0, csign, m->cvec,
+                      m->svec, c->sc->active, nullptr, nullptr));
+  return hop64_batch(c, EPI_XPAY_G5, R_, B64(m->t64, 1, Vh), B64(out, 0, Vh), B64(v, 0, Vh), 0, -k * k, csign,
+                     m->cvec, nullptr, c->sc->active, norm_part, nblk);
 }
 
 template <class P>
@@ -493,8 +639,10 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   using R = typename P::R;
   using FT = FieldTraits<SP>;
   using FA = FieldTraits<AC>;
-  QKX_TRY(mixed_alloc<P>(c, nrhs));
+  QKX_TRY(mixed_alloc<P>(c, nrhs, true));
   MixedState* m = c->mixed;
+  HopTile tile;
+  QKX_TRY(tile_for<P>(c, nrhs, &tile));
   const int Vh = c->Vh;
   const size_t n12 = 12 * (size_t)Vh;
   const size_t hb = sizeof(double2) * n12;
@@ -526,24 +674,35 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     QKX_CUDA(cudaMemcpyAsync(m->bO + i * n12, b[i] + n12, hb, cudaMemcpyDeviceToDevice, c->st));
   }
   k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), m->part);
+  counted(c);
   k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+  counted(c);
   k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), m->part);
+  counted(c);
   k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+  counted(c);
   // t_o = A^-1 b_o
   k_mx_site<SITE_TWIST_INV><<<cg2, 256, 0, c->st>>>(B64(m->bO, 1, Vh), B64(m->t64, 1, Vh), 1, m->cvec, m->svec);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   // z = b_e + k D_eo t_o = b^_e, |b^|^2 -> aux2 ; g5bh = g5 b^_e
-  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY>(c, nrhs, U18, c->geom, B64(m->t64, 1, Vh), B64(m->z64, 0, Vh),
-                                                       B64(m->bE, 0, Vh), 0, k, 0.0, false, m->part, -1)));
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_AUX2, c->sc);
+  int nb64 = 0;
+  QKX_TRY(hop64_batch(c, EPI_XPAY, nrhs, B64(m->t64, 1, Vh), B64(m->z64, 0, Vh), B64(m->bE, 0, Vh), 0, k, 0.0,
+                      m->cvec, nullptr, c->sc->active, m->part, &nb64));
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
+  counted(c);
   k_mx_site<SITE_GAMMA5><<<cg2, 256, 0, c->st>>>(B64(m->z64, 0, Vh), B64(m->g5bh, 0, Vh), 0, nullptr, nullptr);
+  counted(c);
   // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2
-  QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part));
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_R2_INIT, c->sc);
+  QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part, &nb64));
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_R2_INIT, c->sc);
+  counted(c);
   QKX_CUDA(cudaMemsetAsync(m->x64, 0, hb * nrhs, c->st));
   QKX_CUDA(cudaMemsetAsync(m->xs.d, 0, FA::words * 16 * (size_t)Vh * nrhs, c->st));
   k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
+  counted(c);
   k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
   QKX_CUDA(cudaStreamSynchronize(c->st));
@@ -569,14 +728,19 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     }
   }
   const bool graphs = sp->use_graphs != 0;
-  if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || !graphs || prof)) {
+  if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || m->graph_nr != tile.nr ||
+                   m->graph_nt != tile.nt || !graphs || prof)) {
     cudaGraphExecDestroy(m->graph);
     m->graph = nullptr;
   }
   if (graphs && !m->graph) {
     cudaGraph_t gr;
     QKX_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-    int rc = SL::iteration(c, nrhs, prof);
+    c->capturing = 1;
+    c->captured = 0;
+    int rc = SL::iteration(c, nrhs, prof, tile);
+    c->capturing = 0;
+    m->graph_kernels = c->captured;
     cudaError_t e = cudaStreamEndCapture(c->st, &gr);
     if (rc != QKX_OK) return rc;
     if (e != cudaSuccess) {
@@ -587,6 +751,8 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     cudaGraphDestroy(gr);
     m->graph_R = nrhs;
     m->graph_kappa = c->p.kappa;
+    m->graph_nr = tile.nr;
+    m->graph_nt = tile.nt;
   }
 
   const int maxIter = sp->maxIter;
@@ -598,8 +764,9 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     if (!nact) break;
     if (m->graph) {
       QKX_CUDA(cudaGraphLaunch(m->graph, c->st));
+      counted(c, (int)m->graph_kernels);
     } else {
-      QKX_TRY(SL::iteration(c, nrhs, prof));
+      QKX_TRY(SL::iteration(c, nrhs, prof, tile));
     }
     iter++;
     since++;
@@ -630,11 +797,15 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     since = 0;
     // x64 += x_s ; z = g5 b^ - g5 Mh x64 = g5 rhat ; r = Mh^+ rhat
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+    counted(c);
     QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
     k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
+    counted(c);
     k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
-    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part));
-    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nblk, FIN_AUX2, c->sc);
+    counted(c);
+    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb64));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
+    counted(c);
     QKX_CUDA(cudaGetLastError());
     QKX_CUDA(cudaMemcpyAsync(sh->aux, c->sc->aux, 2 * sizeof(double) * MAX_RHS, cudaMemcpyDeviceToHost, c->st));
     QKX_CUDA(cudaStreamSynchronize(c->st));
@@ -654,6 +825,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
     QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
     k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
+    counted(c);
     QKX_CUDA(cudaGetLastError());
   }
   int rc = QKX_OK;
@@ -665,19 +837,24 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
   QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
   if (nact)  // fold what the unconverged RHS accumulated since their last update
-    k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+    {
+      k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+      counted(c);
+    }
   // x_o = A^-1 (b_o + k D_oe x_e) into t64
-  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY_TWINV>(c, nrhs, U18, c->geom, B64(m->x64, 0, Vh),
-                                                             B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0, true,
-                                                             nullptr, -1)));
+  QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
+                      m->cvec, m->svec, c->sc->active, nullptr, nullptr));
   // M x on the full lattice (even half in x64, odd half in t64) into (z64, r64)
-  QKX_TRY((hop_batch<SpinorF64, H18, double, EPI_XPAY>(c, nrhs, U18, c->geom, B64full(m->x64, m->t64, Vh),
-                                                       B64full(m->z64, m->r64, Vh), B64full(m->x64, m->t64, Vh), -1,
-                                                       -k, 1.0, false, nullptr, -1)));
+  QKX_TRY(hop64_batch(c, EPI_XPAY, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->z64, m->r64, Vh),
+                      B64full(m->x64, m->t64, Vh), -1, -k, 1.0, m->cvec, nullptr, c->sc->active, nullptr, nullptr));
   k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), B64(m->z64, 0, Vh), nullptr, m->part);
+  counted(c);
   k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+  counted(c);
   k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), B64(m->r64, 0, Vh), nullptr, m->part);
+  counted(c);
   k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+  counted(c);
   QKX_CUDA(cudaGetLastError());
   for (int i = 0; i < nrhs; i++) {
     QKX_CUDA(cudaMemcpyAsync(x[i], m->x64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
@@ -707,6 +884,46 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   if (rc == QKX_ERR_NOT_CONVERGED)
     set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
   return rc;
+}
+
+// the captured graph holds gauge geometry: drop it when the gauge changes
+void mixed_invalidate(qkx_ctx* c) {
+  MixedState* m = c->mixed;
+  if (m && m->graph) {
+    cudaStreamSynchronize(c->st);
+    cudaGraphExecDestroy(m->graph);
+    m->graph = nullptr;
+  }
+}
+
+int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms) {
+  HopTile t;
+  double best = 0;
+  int rc;
+  if (precision == QKX_PREC_HALF || precision == QKX_PREC_SINGLE) {
+    if (!c->compressible) {
+      set_error("tuning the sloppy hop needs SU(3) links (12-real reconstruction)");
+      return QKX_ERR_UNSUPPORTED;
+    }
+  }
+  if (precision == QKX_PREC_HALF) {
+    QKX_TRY(mixed_alloc<PHalf>(c, nrhs, false));
+    rc = tune_tile<PHalf>(c, nrhs, &t, &best);
+  } else if (precision == QKX_PREC_SINGLE) {
+    QKX_TRY(mixed_alloc<PSingle>(c, nrhs, false));
+    rc = tune_tile<PSingle>(c, nrhs, &t, &best);
+  } else if (precision == QKX_PREC_DOUBLE) {
+    QKX_TRY(mixed_alloc<PDouble>(c, nrhs, false));
+    rc = tune_tile<PDouble>(c, nrhs, &t, &best);
+  } else {
+    set_error("invalid argument: precision");
+    return QKX_ERR_INVALID;
+  }
+  if (rc != QKX_OK) return rc;
+  if (nr) *nr = t.nr;
+  if (nt) *nt = t.nt;
+  if (ms) *ms = best;
+  return QKX_OK;
 }
 
 int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b, double2* const* x,

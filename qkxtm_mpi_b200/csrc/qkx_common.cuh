@@ -67,6 +67,11 @@ template <typename R>
 struct Link {
   Cx<R> m[3][3];
 };
+// the four spins of one colour of a spinor
+template <typename R>
+struct Spin4 {
+  Cx<R> s[4];
+};
 
 // ---------------------------------------------------------------- gamma tables
 // Every gamma matrix used here has one non-zero per row: row r has the entry
@@ -144,6 +149,20 @@ struct Proj {
     }
   }
 
+  // reconstruct() for a single colour: h0, h1 are that colour of the two rows
+  template <typename R>
+  __device__ __forceinline__ static void reconstruct1(Spin4<R>& acc, Cx<R> h0, Cx<R> h1) {
+    if constexpr (diag) {
+      acc.s[drow] = acc.s[drow] + h0;
+      acc.s[drow + 1] = acc.s[drow + 1] + h1;
+    } else {
+      acc.s[0] = acc.s[0] + h0;
+      acc.s[1] = acc.s[1] + h1;
+      acc.s[c0] = acc.s[c0] + phase<q0>(h0);
+      acc.s[c1] = acc.s[c1] + phase<q1>(h1);
+    }
+  }
+
   template <typename R>
   __device__ __forceinline__ static void reconstruct(Spinor<R>& acc, const HalfSpinor<R>& h) {
     if constexpr (diag) {
@@ -186,6 +205,12 @@ __device__ __forceinline__ Spinor<R> gamma5(const Spinor<R>& s) {
     }
   }
   return o;
+}
+
+template <int B, typename R>
+__device__ __forceinline__ Spin4<R> gamma5_4(const Spin4<R>& v) {
+  if constexpr (B == 0) return {{v.s[2], v.s[3], v.s[0], v.s[1]}};
+  else return {{v.s[0], v.s[1], R(-1) * v.s[2], R(-1) * v.s[3]}};
 }
 
 // U h and U^+ h on a half spinor
@@ -262,6 +287,11 @@ struct SpinorF64 {
     }
     return s;
   }
+  static constexpr bool has_norm = false;
+  __device__ __forceinline__ Spinor<double> load_raw(int parity, int cb, double& n) const {
+    n = 1.0;
+    return load(parity, cb);
+  }
   __device__ __forceinline__ void store(int parity, int cb, const Spinor<double>& s) const {
     double2* b = (parity ? p1 : p0) + cb;
 #pragma unroll
@@ -291,6 +321,11 @@ struct SpinorF32 {
       s.c[(2 * q + 1) / 3][(2 * q + 1) % 3] = {f.z, f.w};
     }
     return s;
+  }
+  static constexpr bool has_norm = false;
+  __device__ __forceinline__ Spinor<float> load_raw(int parity, int cb, float& n) const {
+    n = 1.f;
+    return load(parity, cb);
   }
   __device__ __forceinline__ void store(int parity, int cb, const Spinor<float>& s) const {
     float4* b = (parity ? p1 : p0) + cb;
@@ -334,6 +369,26 @@ struct SpinorF16 {
         float2 f = __half22float2(h);
         int idx = 4 * q + k;
         s.c[idx / 3][idx % 3] = {f.x * n, f.y * n};
+      }
+    }
+    return s;
+  }
+  // the stored values without the site scale (the caller multiplies by n later,
+  // after the linear projection and link multiplication)
+  static constexpr bool has_norm = true;
+  __device__ __forceinline__ Spinor<float> load_raw(int parity, int cb, float& n) const {
+    const uint4* b = (parity ? p1 : p0) + cb;
+    n = __ldg((parity ? n1 : n0) + cb);
+    Spinor<float> s;
+#pragma unroll
+    for (int q = 0; q < 3; q++) {
+      uint4 w = __ldg(b + (size_t)q * Vh);
+      uint32_t ws[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+      for (int k = 0; k < 4; k++) {
+        float2 f = __half22float2(*reinterpret_cast<__half2*>(&ws[k]));
+        int idx = 4 * q + k;
+        s.c[idx / 3][idx % 3] = {f.x, f.y};
       }
     }
     return s;

