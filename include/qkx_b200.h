@@ -171,6 +171,24 @@ QKX_API int qkx_X_eq_aX_p_Y(qkx_ctx* ctx, double* x_dev, double a, const double*
 /* Vector::norm2 (lib/lattice_util.cpp:464-477) */
 QKX_API int qkx_norm2(qkx_ctx* ctx, const double* x_dev, double* result);
 
+/* Allocation-free Re sum conj(x) y over n_sites sites (12 complex numbers each)
+ * of two device fields, FP64, result written to *result (host memory) after
+ * the work on `stream` (a cudaStream_t, NULL for the legacy default stream)
+ * has finished.  No counterpart in the reference: it is reCdotXdagY for
+ * callers that cannot allocate device memory -- code running under a fixed
+ * device-memory budget that another allocator already owns, or that must not
+ * enter the allocator on its path -- and therefore cannot create a qkx_ctx.
+ * It calls no cudaMalloc/cudaFree: its scratch (the per-block partial sums)
+ * is a fixed 512 KB array compiled into the library, resident on every GPU
+ * that loads it until the process exits.  Inputs above QKX_NOALLOC_MAX_SITES
+ * sites are rejected with QKX_ERR_INVALID.  The first call on a device looks
+ * up the array's device address (cudaGetSymbolAddress), so make that first
+ * call before any stream capture.  All calls on a device share the array:
+ * calls whose GPU work overlaps (other streams or host threads) race. */
+#define QKX_NOALLOC_MAX_SITES 11184810ULL
+QKX_API int qkx_reCdotXdagY_noalloc(const double* x_dev, const double* y_dev, size_t n_sites, double* result,
+                                    void* stream);
+
 /* ---------------------------------------------------------------- solvers */
 typedef struct qkx_solve_info {
   int iterations;          /* CG iterations (max over right-hand sides) */

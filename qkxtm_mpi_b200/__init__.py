@@ -37,6 +37,7 @@ ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOGAUGE, ERR_NOT_CONVERGED, ERR_NAN, ERR_U
     -1, -2, -3, -4, -5, -6, -7)
 
 LINKS_AS_GIVEN, LINKS_APPLY_BC = 0, 1
+NOALLOC_MAX_SITES = 11184810  # QKX_NOALLOC_MAX_SITES
 SOLVER_CG_FP64, SOLVER_CG_EO_MIXED = 0, 1
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
 
@@ -58,7 +59,7 @@ SYMBOLS = [
     "qkx_get_params", "qkx_sync", "qkx_stream", "qkx_spinor_bytes", "qkx_volume",
     "qkx_load_gauge", "qkx_gauge_generate", "qkx_download_gauge", "qkx_gauge_compressible",
     "qkx_apply", "qkx_apply_dev", "qkx_spinor_upload", "qkx_spinor_download",
-    "qkx_reCdotXdagY", "qkx_X_eq_X_p_aY", "qkx_X_eq_aX_p_Y", "qkx_norm2",
+    "qkx_reCdotXdagY", "qkx_X_eq_X_p_aY", "qkx_X_eq_aX_p_Y", "qkx_norm2", "qkx_reCdotXdagY_noalloc",
     "qkx_cg", "qkx_cg_dev", "qkx_invert", "qkx_invert_dev",
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
@@ -129,6 +130,7 @@ def lib() -> C.CDLL:
         L.qkx_spinor_download.argtypes = [_vp, _vp, _vp]
         L.qkx_reCdotXdagY.argtypes = [_vp, _vp, _vp, _dp]
         L.qkx_norm2.argtypes = [_vp, _vp, _dp]
+        L.qkx_reCdotXdagY_noalloc.argtypes = [_vp, _vp, C.c_size_t, _dp, _vp]
         L.qkx_X_eq_X_p_aY.argtypes = [_vp, _vp, C.c_double, _vp]
         L.qkx_X_eq_aX_p_Y.argtypes = [_vp, _vp, C.c_double, _vp]
         L.qkx_cg.argtypes = [_vp, _vp, _vp, C.POINTER(SolveInfo)]
