@@ -44,8 +44,8 @@ FALLBACK_HBM_GBS = 6650.0
 
 
 def env_rank():
-    return (int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)),
-            int(os.environ.get("LOCAL_RANK", 0)))
+    from qkxtm_mpi_b200.dist import env_rank as er
+    return er()
 
 
 def measured_peak_hbm():
@@ -124,23 +124,21 @@ def point_sources(np, t_src: int):
 def run_ours(args):
     import numpy as np
     import torch
-    import torch.distributed as dist
 
     import qkxtm_mpi_b200 as Q
+    from qkxtm_mpi_b200 import dist as D
 
     rank, world, local = env_rank()
     torch.cuda.set_device(local)
     if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
-                                device_id=torch.device("cuda", local))
+        D.init("nccl", local)
     prec = {"half": Q.PREC_HALF, "single": Q.PREC_SINGLE, "double": Q.PREC_DOUBLE}[args.precision]
     V = L[0] * L[1] * L[2] * L[3]
 
     lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, twistSign=1, boundaryT=-1, tol=TOL,
                                   maxIter=5000), device=local)
     lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
-    t_src = (2 * rank) % L[3]
+    t_src = D.source_timeslice(rank, L[3])
     srcs = point_sources(np, t_src)
     bd = [lat.field(b) for b in srcs]
     xd = [lat.field() for _ in srcs]
@@ -153,9 +151,7 @@ def run_ours(args):
             raise RuntimeError(f"solve did not converge: {info.as_dict()}")
         return info
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
+    barrier = D.barrier
 
     for _ in range(args.warmup):
         solve()
@@ -179,11 +175,7 @@ def run_ours(args):
     launches = lat.kernel_launches() - k0
     hop_n, hop_ms, hop_bytes = lat.profile_read()
     lat.profile(False)
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = D.max_over_ranks(e0.elapsed_time(e1))
     step_s = ms / 1e3 / args.steps
 
     # ---- end to end through the host-buffer C ABI
@@ -208,11 +200,7 @@ def run_ours(args):
     for _ in range(n_e2e):
         e2e_step()
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / n_e2e
-    if world > 1:
-        t = torch.tensor([e2e_s], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = D.max_over_ranks((time.perf_counter() - t0) / n_e2e)
     h2d = Uh.nbytes + sum(b.nbytes for b in bh)
     d2h = sum(x.nbytes for x in xh)
 
@@ -234,8 +222,7 @@ def run_ours(args):
         cpu = {"value": cb["value"], "unit": "s", "cores": cb["cores"], "kind": cb["kind"],
                "sample": cb["sample"]}
 
-    if world > 1:
-        dist.destroy_process_group()
+    D.finish()
     if rank != 0:
         return
 

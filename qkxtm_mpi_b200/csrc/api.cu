@@ -85,6 +85,16 @@ int ensure_stage(qkx_ctx* c) {
   return QKX_OK;
 }
 
+int ensure_links(qkx_ctx* c) {
+  if (c->U18) return QKX_OK;
+  cudaError_t e = cudaMalloc(&c->U18, sizeof(double2) * 36 * c->V);
+  if (e != cudaSuccess) {
+    set_error("gauge field: %s", cudaGetErrorString(e));
+    return QKX_ERR_NOMEM;
+  }
+  return QKX_OK;
+}
+
 int ensure_work(qkx_ctx* c) {
   for (int i = 0; i < qkx_ctx::NW; i++) {
     if (c->w[i]) continue;
@@ -454,8 +464,18 @@ int qkx_create(const qkx_params* p, int device, qkx_ctx** out) {
   };
   cudaError_t e;
   if ((e = cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking)) != cudaSuccess) fail(e, "stream");
+  // The host-buffer entry points stage their device copies through the
+  // stream-ordered allocator; keep freed blocks in this process's pool instead
+  // of returning them to the driver at every synchronisation, so repeated
+  // calls do not pay for fresh allocations.
+  if (rc == QKX_OK) {
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;
+      cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+  }
   const size_t fbytes = sizeof(double2) * 12 * c->V;
-  if (rc == QKX_OK && (e = cudaMalloc(&c->U18, sizeof(double2) * 36 * c->V)) != cudaSuccess) fail(e, "links");
   (void)fbytes;  // the staging buffer and the FP64 work fields are allocated on first use
   c->npart = std::max(148 * 8, 2 * (int)((c->Vh + 31) / 32)) + 1;  // room for any hop block size >= 32
   if (rc == QKX_OK && (e = cudaMalloc(&c->part, sizeof(double) * c->npart)) != cudaSuccess) fail(e, "partials");
@@ -531,6 +551,7 @@ int qkx_load_gauge(qkx_ctx* c, const double* U_host, int bc_mode) {
   if (!c || !U_host) return invalid("NULL argument");
   if (bc_mode != QKX_LINKS_AS_GIVEN && bc_mode != QKX_LINKS_APPLY_BC) return invalid("bc_mode");
   QKX_CUDA(cudaSetDevice(c->device));
+  QKX_TRY(ensure_links(c));
   double2* tmp = nullptr;
   const size_t bytes = sizeof(double2) * 36 * c->V;
   QKX_CUDA(cudaMallocAsync(&tmp, bytes, c->st));
@@ -547,6 +568,7 @@ int qkx_gauge_generate(qkx_ctx* c, double eps, unsigned long long seed, int bc_m
   if (!c) return invalid("ctx is NULL");
   if (bc_mode != QKX_LINKS_AS_GIVEN && bc_mode != QKX_LINKS_APPLY_BC) return invalid("bc_mode");
   QKX_CUDA(cudaSetDevice(c->device));
+  QKX_TRY(ensure_links(c));
   const int nl = 8 * c->Vh;
   k_gauge_generate<<<(nl + 127) / 128, 128, 0, c->st>>>(c->U18, c->geom, eps, seed);
   counted(c);

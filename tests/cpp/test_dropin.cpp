@@ -1,0 +1,114 @@
+// test_dropin.cpp -- the reference's driver flow (bin/test_applyTM.cpp,
+// bin/test_invert.cpp) written against include/qkxTM_b200.hpp, checked
+// against the CPU oracle.  Built and run by tests/test_gpu_dropin.py.
+#include <cmath>
+#include <cstdio>
+
+#include "../../include/qkxTM_b200.hpp"
+#include "../../oracle/qkx_oracle.h"
+
+using namespace qkxTM_b200;
+
+static double rel(const double* a, const double* b, long n) {
+  double d = 0, s = 0;
+  for (long i = 0; i < n; i++) {
+    d += (a[i] - b[i]) * (a[i] - b[i]);
+    s += b[i] * b[i];
+  }
+  return std::sqrt(d / (s > 0 ? s : 1));
+}
+
+int main() {
+  LatticeInfo latInfo;
+  latInfo.L[0] = 8;
+  latInfo.L[1] = 8;
+  latInfo.L[2] = 8;
+  latInfo.L[3] = 16;
+  latInfo.kappa = 0.16;
+  latInfo.mu = 0.01;
+  latInfo.twistSign = +1;
+  latInfo.tol = 1e-10;
+  latInfo.maxIter = 1000;
+  latInfo.boundaryT = -1;
+
+  Gauge* gauge = new Gauge(&latInfo);
+  Vector* vec = new Vector(&latInfo);
+  Vector* vecIn = new Vector(&latInfo);
+  Vector* tmp = new Vector(&latInfo);
+  const long V = vec->lV4d;
+  int fails = 0;
+
+  orc_gauge_random(latInfo.L, 0.3, 1234, reinterpret_cast<double*>(gauge->M));
+  gauge->applyBoundaryCondition(&latInfo);
+  orc_spinor_gaussian(latInfo.L, 42, vecIn->data());
+
+  orc_params op = {{8, 8, 8, 16}, latInfo.kappa, latInfo.mu, latInfo.twistSign, latInfo.boundaryT, latInfo.tol, 1000};
+  std::vector<double> ref(24 * V);
+  const double* U = reinterpret_cast<const double*>(gauge->M);
+
+  vec->tm(*vecIn, *gauge, &latInfo);
+  orc_tm(&op, U, vecIn->data(), ref.data(), ORC_UKQCD);
+  double e = rel(vec->data(), ref.data(), 24 * V);
+  printf("tm            rel err %.2e\n", e);
+  fails += e > 1e-13;
+
+  vec->tm_xxDagTm_xx(*vecIn, *gauge, &latInfo, OO);
+  orc_tm_xx_dagtm_xx(&op, U, vecIn->data(), ref.data(), ORC_OO, ORC_UKQCD);
+  e = rel(vec->data(), ref.data(), 24 * V);
+  printf("tm_xxDagTm_xx rel err %.2e\n", e);
+  fails += e > 1e-13;
+
+  vec->tm_xx_chiral(*vecIn, *gauge, &latInfo, EE);
+  orc_tm_xx(&op, U, vecIn->data(), ref.data(), ORC_EE, ORC_CHIRAL);
+  e = rel(vec->data(), ref.data(), 24 * V);
+  printf("tm_xx_chiral  rel err %.2e\n", e);
+  fails += e > 1e-13;
+
+  // BLAS with the reference signatures
+  double d = reCdotXdagY(*vecIn, *vecIn);
+  double dref = orc_re_dot(V, vecIn->data(), vecIn->data());
+  printf("reCdotXdagY   rel err %.2e\n", std::fabs(d - dref) / dref);
+  fails += std::fabs(d - dref) > 1e-12 * dref;
+
+  // bin/test_invert.cpp:95-117: in = M^+ b ; CG on M^+M with x zeroed
+  Vector* vec_out = new Vector(&latInfo);
+  tmp->tmDag(*vecIn, *gauge, &latInfo);
+  vec_out->zero();
+  CG cg(&latInfo, *gauge);
+  qkx_solve_info info = cg(*vec_out, *tmp, &latInfo);
+  std::vector<double> xo(24 * V, 0.0);
+  orc_tm_dag(&op, U, vecIn->data(), ref.data(), ORC_UKQCD);
+  int it = orc_cg(&op, U, ref.data(), xo.data(), nullptr, 0);
+  e = rel(vec_out->data(), xo.data(), 24 * V);
+  printf("CG            iterations %d (oracle %d), solution rel err %.2e\n", info.iterations, it, e);
+  fails += e > 1e-9 || std::abs(info.iterations - it) > 1;
+
+  // the batched B200 solve of M x = b
+  std::vector<Vector*> bs = {vecIn}, xs = {vec};
+  qkx_solve_info inv = cg.invert(bs, xs, &latInfo);
+  vec_out->tm(*vec, *gauge, &latInfo);
+  double r2 = 0, b2 = 0;
+  for (long i = 0; i < 24 * V; i++) {
+    double dv = vecIn->data()[i] - vec_out->data()[i];
+    r2 += dv * dv;
+    b2 += vecIn->data()[i] * vecIn->data()[i];
+  }
+  printf("invert        true residual %.2e (library %.2e)\n", std::sqrt(r2 / b2), inv.true_residual);
+  fails += std::sqrt(r2 / b2) > 1e-10;
+
+  // errors are exceptions carrying the status code
+  try {
+    vec->tm_xx(*vecIn, *gauge, &latInfo, EO);
+    fails++;
+  } catch (const Error& err) {
+    printf("wrong parity  -> Error %d\n", err.code);
+  }
+
+  delete vec_out;
+  delete tmp;
+  delete vecIn;
+  delete vec;
+  delete gauge;
+  printf(fails ? "FAILED %d\n" : "OK\n", fails);
+  return fails ? 1 : 0;
+}

@@ -88,3 +88,9 @@ def test_create_without_gpu_fails_cleanly(built_lib):
     with pytest.raises(Q.QkxError) as e:
         Q.Lattice(Q.LatticeInfo(L=(4, 4, 4, 4)))
     assert e.value.code == Q.ERR_CUDA
+
+
+def test_cpp_dropin_header_compiles():
+    """include/qkxTM_b200.hpp (the reference-named C++ layer) is valid C++17."""
+    src = os.path.join(ROOT, "tests", "cpp", "test_dropin.cpp")
+    subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src], check=True)
