@@ -433,7 +433,7 @@ static int check_params(const qkx_params* p) {
     if (p->L[i] < 2) return invalid("lattice extents must be >= 2");
   if (p->L[0] % 2) return invalid("L[0] must be even for the even-odd layout");
   long long V = (long long)p->L[0] * p->L[1] * p->L[2] * p->L[3];
-  if (V > (1LL << 30)) return invalid("lattice volume above 2^30 sites");
+  if (V > (1LL << 28)) return invalid("lattice volume above 2^28 sites (32-bit site-word indexing)");
   if (p->twistSign != 1 && p->twistSign != -1) return invalid("twistSign must be +1 or -1");
   if (p->boundaryT != 1 && p->boundaryT != -1) return invalid("boundaryT must be +1 or -1");
   if (!(p->kappa == p->kappa) || !(p->mu == p->mu)) return invalid("kappa/mu is NaN");

@@ -1,10 +1,11 @@
 // hop_mrhs.cuh -- the hopping term for a batch of right-hand sides with NR of
 // them per thread: each thread computes one output site for NR right-hand
 // sides, so every link is loaded, converted and rebuilt from its 12 reals once
-// and applied to NR spinors.  The FP16 site scale is applied after the
-// projection and link multiplication (both linear), on 6 instead of 12
-// complex numbers.  Neighbours are found from the lexicographic index with
-// one add and a wrap test per direction.
+// and applied to NR spinors.  The FP16 site scale (and the boundary sign) is
+// applied after the projection and link multiplication (both linear), folded
+// into the FMAs that accumulate the rebuilt spinor.  Neighbours are found from
+// the lexicographic index with one add and a wrap test per direction, and each
+// right-hand side's base pointers are formed once per thread.
 //
 // Same operator and epilogues as hop.cuh (reference Vector::applyDslash,
 // lib/lattice_util.cpp:1158-1213, with the twist site factors of
@@ -12,7 +13,7 @@
 //
 // Grid: blockIdx.x = site_block * ngroups + group, group g covering the
 // right-hand sides [g*NR, g*NR + NR) of the batch.  (NR, NT) are chosen per
-// lattice and batch by the autotuner (tune.cu).
+// lattice and batch by the autotuner (tune_tile in mixed.cu).
 #pragma once
 #include "hop.cuh"
 
@@ -39,8 +40,8 @@ __device__ __forceinline__ void block_partials(const double (&v)[NR], double* pa
 }
 
 template <int NR, class SP, class GA, typename R, int B, bool DAG, int MU>
-__device__ __forceinline__ void hop_dir_m(const SP& in, const GA& gauge, const Geom& g, int par, int cb,
-                                          const int x[4], int s, int stride, int r0, const bool (&act)[NR],
+__device__ __forceinline__ void hop_dir_m(const SP (&in)[NR], const GA& gauge, const Geom& g, int par, int cb,
+                                          const int x[4], int s, int stride, const bool (&act)[NR],
                                           Spinor<R> (&acc)[NR]) {
   constexpr int SF = DAG ? +1 : -1;  // forward projector 1 + SF*g
   const int Lm = g.L[MU];
@@ -52,16 +53,11 @@ __device__ __forceinline__ void hop_dir_m(const SP& in, const GA& gauge, const G
     for (int j = 0; j < NR; j++) {
       if (!act[j]) continue;
       R nrm;
-      const Spinor<R> v = in.shift(r0 + j).load_raw(1 - par, n, nrm);
+      const Spinor<R> v = in[j].load_raw(1 - par, n, nrm);
       HalfSpinor<R> h, uh;
       Proj<B, MU, SF>::project(v, h);
       mul_link(u, h, uh);
-      if (SP::has_norm || flip) {
-        const R f = flip ? -nrm : nrm;
-#pragma unroll
-        for (int k = 0; k < 6; k++) uh.c[k / 3][k % 3] = f * uh.c[k / 3][k % 3];
-      }
-      Proj<B, MU, SF>::reconstruct(acc[j], uh);
+      Proj<B, MU, SF>::reconstruct_scaled(acc[j], uh, flip ? -nrm : nrm);
     }
   }
   {
@@ -72,16 +68,11 @@ __device__ __forceinline__ void hop_dir_m(const SP& in, const GA& gauge, const G
     for (int j = 0; j < NR; j++) {
       if (!act[j]) continue;
       R nrm;
-      const Spinor<R> v = in.shift(r0 + j).load_raw(1 - par, n, nrm);
+      const Spinor<R> v = in[j].load_raw(1 - par, n, nrm);
       HalfSpinor<R> h, uh;
       Proj<B, MU, -SF>::project(v, h);
       mul_link_dag(u, h, uh);
-      if (SP::has_norm || flip) {
-        const R f = flip ? -nrm : nrm;
-#pragma unroll
-        for (int k = 0; k < 6; k++) uh.c[k / 3][k % 3] = f * uh.c[k / 3][k % 3];
-      }
-      Proj<B, MU, -SF>::reconstruct(acc[j], uh);
+      Proj<B, MU, -SF>::reconstruct_scaled(acc[j], uh, flip ? -nrm : nrm);
     }
   }
 }
@@ -114,13 +105,16 @@ __global__ void __launch_bounds__(NT) hop_mrhs_kernel(HopArgs<SP, GA> A) {
     cb_coords(A.g, cb, par, x);
     const int L0 = A.g.L[0], L01 = L0 * A.g.L[1], L012 = L01 * A.g.L[2];
     const int s = x[0] + L0 * x[1] + L01 * x[2] + L012 * x[3];
+    SP in[NR];  // each right-hand side's input, shifted once per thread
+#pragma unroll
+    for (int j = 0; j < NR; j++) in[j] = A.in.shift(r0 + j);
     Spinor<R> acc[NR];
 #pragma unroll
     for (int j = 0; j < NR; j++) zero(acc[j]);
-    hop_dir_m<NR, SP, GA, R, B, DAG, 0>(A.in, A.gauge, A.g, par, cb, x, s, 1, r0, act, acc);
-    hop_dir_m<NR, SP, GA, R, B, DAG, 1>(A.in, A.gauge, A.g, par, cb, x, s, L0, r0, act, acc);
-    hop_dir_m<NR, SP, GA, R, B, DAG, 2>(A.in, A.gauge, A.g, par, cb, x, s, L01, r0, act, acc);
-    hop_dir_m<NR, SP, GA, R, B, DAG, 3>(A.in, A.gauge, A.g, par, cb, x, s, L012, r0, act, acc);
+    hop_dir_m<NR, SP, GA, R, B, DAG, 0>(in, A.gauge, A.g, par, cb, x, s, 1, act, acc);
+    hop_dir_m<NR, SP, GA, R, B, DAG, 1>(in, A.gauge, A.g, par, cb, x, s, L0, act, acc);
+    hop_dir_m<NR, SP, GA, R, B, DAG, 2>(in, A.gauge, A.g, par, cb, x, s, L01, act, acc);
+    hop_dir_m<NR, SP, GA, R, B, DAG, 3>(in, A.gauge, A.g, par, cb, x, s, L012, act, acc);
 
     const R a = R(A.a);
 #pragma unroll

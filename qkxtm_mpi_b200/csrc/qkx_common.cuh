@@ -46,6 +46,12 @@ __device__ __forceinline__ Cx<R> cmulc(Cx<R> a, Cx<R> b) {
 template <typename R>
 __device__ __forceinline__ Cx<R> conj(Cx<R> a) { return {a.re, -a.im}; }
 
+// f * a + b for a real scale f
+template <typename R>
+__device__ __forceinline__ Cx<R> fma_s(R f, Cx<R> a, Cx<R> b) {
+  return {fma(f, a.re, b.re), fma(f, a.im, b.im)};
+}
+
 // multiply by a phase code: 0 -> 1, 1 -> i, 2 -> -1, 3 -> -i
 template <int PH, typename R>
 __device__ __forceinline__ Cx<R> phase(Cx<R> z) {
@@ -160,6 +166,26 @@ struct Proj {
       acc.s[1] = acc.s[1] + h1;
       acc.s[c0] = acc.s[c0] + phase<q0>(h0);
       acc.s[c1] = acc.s[c1] + phase<q1>(h1);
+    }
+  }
+
+  // acc += f * (rebuilt spinor): the scale is folded into the accumulating FMAs
+  template <typename R>
+  __device__ __forceinline__ static void reconstruct_scaled(Spinor<R>& acc, const HalfSpinor<R>& h, R f) {
+    if constexpr (diag) {
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        acc.c[drow][a] = fma_s(f, h.c[0][a], acc.c[drow][a]);
+        acc.c[drow + 1][a] = fma_s(f, h.c[1][a], acc.c[drow + 1][a]);
+      }
+    } else {
+#pragma unroll
+      for (int a = 0; a < 3; a++) {
+        acc.c[0][a] = fma_s(f, h.c[0][a], acc.c[0][a]);
+        acc.c[1][a] = fma_s(f, h.c[1][a], acc.c[1][a]);
+        acc.c[c0][a] = fma_s(f, phase<q0>(h.c[0][a]), acc.c[c0][a]);
+        acc.c[c1][a] = fma_s(f, phase<q1>(h.c[1][a]), acc.c[c1][a]);
+      }
     }
   }
 
@@ -282,7 +308,7 @@ struct SpinorF64 {
     Spinor<double> s;
 #pragma unroll
     for (int k = 0; k < 12; k++) {
-      double2 d = __ldg(b + (size_t)k * Vh);
+      double2 d = __ldg(b + k * Vh);
       s.c[k / 3][k % 3] = {d.x, d.y};
     }
     return s;
@@ -295,7 +321,7 @@ struct SpinorF64 {
   __device__ __forceinline__ void store(int parity, int cb, const Spinor<double>& s) const {
     double2* b = (parity ? p1 : p0) + cb;
 #pragma unroll
-    for (int k = 0; k < 12; k++) b[(size_t)k * Vh] = make_double2(s.c[k / 3][k % 3].re, s.c[k / 3][k % 3].im);
+    for (int k = 0; k < 12; k++) b[k * Vh] = make_double2(s.c[k / 3][k % 3].re, s.c[k / 3][k % 3].im);
   }
 };
 
@@ -316,7 +342,7 @@ struct SpinorF32 {
     Spinor<float> s;
 #pragma unroll
     for (int q = 0; q < 6; q++) {
-      float4 f = __ldg(b + (size_t)q * Vh);
+      float4 f = __ldg(b + q * Vh);
       s.c[(2 * q) / 3][(2 * q) % 3] = {f.x, f.y};
       s.c[(2 * q + 1) / 3][(2 * q + 1) % 3] = {f.z, f.w};
     }
@@ -332,7 +358,7 @@ struct SpinorF32 {
 #pragma unroll
     for (int q = 0; q < 6; q++) {
       Cx<float> a = s.c[(2 * q) / 3][(2 * q) % 3], c = s.c[(2 * q + 1) / 3][(2 * q + 1) % 3];
-      b[(size_t)q * Vh] = make_float4(a.re, a.im, c.re, c.im);
+      b[q * Vh] = make_float4(a.re, a.im, c.re, c.im);
     }
   }
 };
@@ -361,7 +387,7 @@ struct SpinorF16 {
     Spinor<float> s;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      uint4 w = __ldg(b + (size_t)q * Vh);
+      uint4 w = __ldg(b + q * Vh);
       uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -382,7 +408,7 @@ struct SpinorF16 {
     Spinor<float> s;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      uint4 w = __ldg(b + (size_t)q * Vh);
+      uint4 w = __ldg(b + q * Vh);
       uint32_t ws[4] = {w.x, w.y, w.z, w.w};
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -411,7 +437,7 @@ struct SpinorF16 {
         __half2 h = __floats2half2_rn(s.c[idx / 3][idx % 3].re * inv, s.c[idx / 3][idx % 3].im * inv);
         ws[k] = *reinterpret_cast<uint32_t*>(&h);
       }
-      b[(size_t)q * Vh] = make_uint4(ws[0], ws[1], ws[2], ws[3]);
+      b[q * Vh] = make_uint4(ws[0], ws[1], ws[2], ws[3]);
     }
     (parity ? n1 : n0)[cb] = m;
   }
@@ -423,11 +449,11 @@ struct GaugeF64x18 {
   const double2* p;
   int Vh;
   __device__ __forceinline__ Link<double> load(int parity, int mu, int cb) const {
-    const double2* b = p + ((size_t)parity * 4 + mu) * 9 * Vh + cb;
+    const double2* b = p + ((parity * 4 + mu) * 9 * Vh + cb);
     Link<double> u;
 #pragma unroll
     for (int k = 0; k < 9; k++) {
-      double2 d = __ldg(b + (size_t)k * Vh);
+      double2 d = __ldg(b + k * Vh);
       u.m[k / 3][k % 3] = {d.x, d.y};
     }
     return u;
@@ -447,11 +473,11 @@ struct GaugeF64x12 {
   const double2* p;
   int Vh;
   __device__ __forceinline__ Link<double> load(int parity, int mu, int cb) const {
-    const double2* b = p + ((size_t)parity * 4 + mu) * 6 * Vh + cb;
+    const double2* b = p + ((parity * 4 + mu) * 6 * Vh + cb);
     Link<double> u;
 #pragma unroll
     for (int k = 0; k < 6; k++) {
-      double2 d = __ldg(b + (size_t)k * Vh);
+      double2 d = __ldg(b + k * Vh);
       u.m[k / 3][k % 3] = {d.x, d.y};
     }
     rebuild_row2(u);
@@ -464,11 +490,11 @@ struct GaugeF32x12 {
   const float4* p;
   int Vh;
   __device__ __forceinline__ Link<float> load(int parity, int mu, int cb) const {
-    const float4* b = p + ((size_t)parity * 4 + mu) * 3 * Vh + cb;
+    const float4* b = p + ((parity * 4 + mu) * 3 * Vh + cb);
     Link<float> u;
 #pragma unroll
     for (int q = 0; q < 3; q++) {
-      float4 f = __ldg(b + (size_t)q * Vh);
+      float4 f = __ldg(b + q * Vh);
       u.m[(2 * q) / 3][(2 * q) % 3] = {f.x, f.y};
       u.m[(2 * q + 1) / 3][(2 * q + 1) % 3] = {f.z, f.w};
     }
@@ -483,7 +509,7 @@ struct GaugeF16x12 {
   const uint2* b;
   int Vh;
   __device__ __forceinline__ Link<float> load(int parity, int mu, int cb) const {
-    size_t o = ((size_t)parity * 4 + mu) * Vh + cb;
+    const int o = (parity * 4 + mu) * Vh + cb;
     uint4 w = __ldg(a + o);
     uint2 v = __ldg(b + o);
     uint32_t ws[6] = {w.x, w.y, w.z, w.w, v.x, v.y};
