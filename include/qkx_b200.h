@@ -247,6 +247,70 @@ QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, 
 QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread, int* threads_per_block,
                      double* ms_per_hop);
 
+/* ---------------------------------------------------------------- gauge-side stencils
+ * The smearing links are a second FP64 gauge field held by the context, used
+ * only by the Gaussian smearing: they are set by qkx_ape_smear or
+ * qkx_load_smearing_gauge and are independent of the operator's links. */
+#define QKX_LINKS_OPERATOR 0   /* the links of qkx_load_gauge / qkx_gauge_generate, as stored */
+#define QKX_LINKS_SMEARING 1   /* the smearing links */
+
+/* Gauge::calculatePlaquette() (lib/lattice_util.cpp:923-946): the mean over
+ * sites and the six planes of Re tr U_mu U_nu U_mu^+ U_nu^+ / 3, for the host
+ * links U_host (Gauge::M layout, taken as given). */
+QKX_API int qkx_plaquette(qkx_ctx* ctx, const double* U_host, double* plaquette);
+/* The same for a field the context holds (QKX_LINKS_OPERATOR includes the
+ * boundary sign when it was applied at load time). */
+QKX_API int qkx_plaquette_loaded(qkx_ctx* ctx, int which, double* plaquette);
+
+/* qcd_projectSU33d(Gauge&) (lib/blas.cpp:6-404): projects the spatial links
+ * (mu = 0, 1, 2) of the host field U_host to SU(3) in place; t-links unchanged. */
+QKX_API int qkx_project_su3(qkx_ctx* ctx, double* U_host);
+
+/* this->APE_smearing(U_tmp, &li) (lib/lattice_util.cpp:948-1078) with U_tmp =
+ * U_in, li.NsmearAPE = nsmear, li.alphaAPE = alpha: nsmear iterations of
+ * U_mu <- P_SU3[U_mu + alpha * (sum of the four spatial staples)] on the
+ * spatial links; the t-links are those of U_in.  The result becomes the
+ * context's smearing links and, if U_out is not NULL, is written to U_out.
+ * U_in is left unchanged (the reference overwrites U_tmp).  nsmear == 0 does
+ * nothing, as in the reference. */
+QKX_API int qkx_ape_smear(qkx_ctx* ctx, const double* U_in, double* U_out, int nsmear, double alpha);
+/* Set the smearing links from host links (Gauge::M layout, as given). */
+QKX_API int qkx_load_smearing_gauge(qkx_ctx* ctx, const double* U_host);
+
+/* this->Gaussian_smearing(vec_tmp, gauge, &li) (lib/lattice_util.cpp:1080-1145)
+ * for nrhs vectors at once, vec_tmp = in[i], gauge = the smearing links:
+ * nsmear iterations of psi <- (psi + alpha sum_{mu<3} [U_mu(x) psi(x+mu) +
+ * U_mu(x-mu)^+ psi(x-mu)]) / (1 + 6 alpha).  Host buffers in Vector::M layout.
+ * The inputs are left unchanged (the reference overwrites vec_tmp).  nsmear
+ * == 0 leaves out untouched, as in the reference. */
+QKX_API int qkx_gaussian_smear(qkx_ctx* ctx, int nrhs, const double* const* in_host, double* const* out_host,
+                               int nsmear, double alpha);
+/* The same on device fields in the even-odd layout; in[i] != out[j] for all i, j. */
+QKX_API int qkx_gaussian_smear_dev(qkx_ctx* ctx, int nrhs, const double* const* in_dev, double* const* out_dev,
+                                   int nsmear, double alpha);
+
+/* ---------------------------------------------------------------- propagators
+ * A propagator is double[V][4 mu][4 nu][3 c1][3 c2][2] (Propagator::M,
+ * include/lattice_util.h:168), site order LEXIC; V*2304 bytes. */
+
+/* Propagator::absorbVector(phi, nu, c2) (lib/lattice_util.cpp:2073-2081):
+ * prop[x][mu][nu][c1][c2] = phi[x][mu][c1] for every x, mu, c1 (host buffers). */
+QKX_API int qkx_propagator_absorb(qkx_ctx* ctx, const double* phi_host, int nu, int c2, double* prop_host);
+
+/* The smeared-source propagator of bin/test_invert_prop.cpp:83-97 in one call:
+ * for the 12 spin-colour point sources at x_src (coordinates x y z t) it
+ * Gaussian-smears the sources (nsmear, alpha, with the smearing links), solves
+ * M x = b for all 12 at once with sp, smears the 12 solutions and assembles
+ * them as prop[.][.][nu][.][c2] = solution of source (nu, c2).  The reference
+ * solves each source with tmDag + CG; here sp->method picks the solver and
+ * sp->tol bounds the true residual.  nsmear == 0 uses unsmeared sources and
+ * sinks.  info receives the solve's aggregate. */
+QKX_API int qkx_propagator(qkx_ctx* ctx, const qkx_solver_params* sp, int nsmear, double alpha, const int x_src[4],
+                           double* prop_host, qkx_solve_info* info);
+/* The same with the propagator written to device memory (V*2304 bytes, host layout). */
+QKX_API int qkx_propagator_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nsmear, double alpha,
+                               const int x_src[4], double* prop_dev, qkx_solve_info* info);
+
 /* ---------------------------------------------------------------- memory helpers */
 /* Page-locked host memory for fast transfers (cudaHostAlloc); NULL on failure. */
 QKX_API void* qkx_host_alloc(size_t bytes);

@@ -89,6 +89,12 @@ def lib():
         L.orc_axpy.argtypes = [C.c_long, C.c_double, _dp, _dp]
         L.orc_xpay.argtypes = [C.c_long, C.c_double, _dp, _dp]
         L.orc_cg.restype = C.c_int
+        L.orc_plaquette_ref.argtypes = [_ip, _dp]
+        L.orc_plaquette_ref.restype = C.c_double
+        L.orc_su3_project_many.argtypes = [C.c_long, _dp]
+        L.orc_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
+        L.orc_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
+        L.orc_absorb_vector.argtypes = [C.c_long, _dp, C.c_int, C.c_int, _dp]
     return _lib
 
 
@@ -107,6 +113,14 @@ def ref():
         _ref.ref_cg.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                 _dp, _dp, _dp]
         _ref.ref_apply_bc.argtypes = [_ip, C.c_int, _dp]
+        _ref.ref_plaquette.argtypes = [_ip, _dp]
+        _ref.ref_plaquette.restype = C.c_double
+        _ref.ref_project_su3.argtypes = [_ip, _dp]
+        _ref.ref_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
+        _ref.ref_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
+        _ref.ref_absorb_vector.argtypes = [_ip, _dp, C.c_int, C.c_int, _dp]
+        _ref.ref_propagator.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
+                                        _dp, _dp, C.c_int, C.c_double, C.c_long, _dp]
     return _ref
 
 
@@ -243,3 +257,72 @@ def ref_cg(L, U, b, kappa, mu, twistSign=1, tol=1e-10, maxIter=1000, x0=None):
 def rel_err(a, b) -> float:
     nb = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))
+
+
+# ---------------------------------------------------------------- smearing / propagator
+def plaquette_ref(L, U) -> float:
+    """Gauge::calculatePlaquette restated (lib/lattice_util.cpp:923)."""
+    return lib().orc_plaquette_ref(_L(L), _ptr(np.ascontiguousarray(U)))
+
+
+def su3_project(m) -> np.ndarray:
+    """qcd_projectSU33d restated (lib/blas.cpp:6) on a stack of 3x3 matrices [..., 3, 3, 2]."""
+    m = np.ascontiguousarray(m, dtype=np.float64).copy()
+    lib().orc_su3_project_many(m.size // 18, _ptr(m))
+    return m
+
+
+def ape_smear(L, U, nsmear, alpha, out=None) -> np.ndarray:
+    """Gauge::APE_smearing restated (lib/lattice_util.cpp:948)."""
+    out = np.zeros_like(U) if out is None else out.copy()
+    lib().orc_ape_smear(_L(L), _ptr(np.ascontiguousarray(U)), _ptr(out), nsmear, alpha)
+    return out
+
+
+def gaussian_smear(L, U, psi, nsmear, alpha, out=None) -> np.ndarray:
+    """Vector::Gaussian_smearing restated (lib/lattice_util.cpp:1080)."""
+    out = np.zeros_like(psi) if out is None else out.copy()
+    lib().orc_gaussian_smear(_L(L), _ptr(np.ascontiguousarray(U)), _ptr(np.ascontiguousarray(psi)),
+                             _ptr(out), nsmear, alpha)
+    return out
+
+
+def absorb_vector(phi, nu, c2, prop) -> None:
+    """Propagator::absorbVector restated (lib/lattice_util.cpp:2073), prop updated in place."""
+    lib().orc_absorb_vector(phi.shape[0], _ptr(np.ascontiguousarray(phi)), nu, c2, _ptr(prop))
+
+
+def ref_plaquette(L, U) -> float:
+    return ref().ref_plaquette(_L(L), _ptr(np.ascontiguousarray(U)))
+
+
+def ref_project_su3(L, U) -> np.ndarray:
+    U = np.ascontiguousarray(U, dtype=np.float64).copy()
+    ref().ref_project_su3(_L(L), _ptr(U))
+    return U
+
+
+def ref_ape_smear(L, U, nsmear, alpha, out=None) -> np.ndarray:
+    out = np.zeros_like(U) if out is None else out.copy()
+    ref().ref_ape_smear(_L(L), _ptr(np.ascontiguousarray(U)), _ptr(out), nsmear, alpha)
+    return out
+
+
+def ref_gaussian_smear(L, U, psi, nsmear, alpha, out=None) -> np.ndarray:
+    out = np.zeros_like(psi) if out is None else out.copy()
+    ref().ref_gaussian_smear(_L(L), _ptr(np.ascontiguousarray(U)), _ptr(np.ascontiguousarray(psi)),
+                             _ptr(out), nsmear, alpha)
+    return out
+
+
+def ref_absorb_vector(L, phi, nu, c2, prop) -> None:
+    ref().ref_absorb_vector(_L(L), _ptr(np.ascontiguousarray(phi)), nu, c2, _ptr(prop))
+
+
+def ref_propagator(L, U, U_smear, kappa, mu, nsmear, alpha, src=0, twistSign=1, tol=1e-10,
+                   maxIter=1000) -> np.ndarray:
+    """The propagator loop of bin/test_invert_prop.cpp:83-97 run by the reference."""
+    prop = np.zeros((volume(L), 4, 4, 3, 3, 2))
+    ref().ref_propagator(_L(L), kappa, mu, twistSign, tol, maxIter, _ptr(np.ascontiguousarray(U)),
+                         _ptr(np.ascontiguousarray(U_smear)), nsmear, alpha, src, _ptr(prop))
+    return prop

@@ -74,6 +74,19 @@ double orc_norm2(long V, const double* x);
 int orc_cg(const orc_params* p, const double* U, const double* in, double* x,
            double* r2_trace, int max_trace);
 
+/* gauge-side stencils and propagator workflow (qkx_oracle_smear.c):
+ * Gauge::calculatePlaquette (lib/lattice_util.cpp:923), qcd_projectSU33d
+ * (lib/blas.cpp:6) on n matrices in place, Gauge::APE_smearing (:948),
+ * Vector::Gaussian_smearing (:1080), Propagator::absorbVector (:2073).
+ * A propagator is [V][4 mu][4 nu][3 c1][3 c2] complex double
+ * (Propagator::M, include/lattice_util.h:168). */
+double orc_plaquette_ref(const int L[4], const double* U);
+void orc_su3_project_many(long n, double* m);
+void orc_ape_smear(const int L[4], const double* U_in, double* U_out, int nsmear, double alpha);
+void orc_gaussian_smear(const int L[4], const double* U, const double* in, double* out, int nsmear,
+                        double alpha);
+void orc_absorb_vector(long V, const double* phi, int nu, int c2, double* prop);
+
 #ifdef __cplusplus
 }
 #endif

@@ -2,7 +2,9 @@
  * ref_shim.cpp -- C entry points around the reference's own classes, compiled
  * together with the unmodified reference sources into oracle/_ref/libqkxref.so.
  * TEST INFRASTRUCTURE ONLY: it lets the tests run the reference's Vector::tm,
- * tm_xx, chiral variants, BLAS and CG::operator() on plain arrays so the CPU
+ * tm_xx, chiral variants, BLAS, CG::operator(), the plaquette, APE and
+ * Gaussian smearing, Propagator::absorbVector and the propagator loop of
+ * bin/test_invert_prop.cpp on plain arrays so the CPU
  * restatement (oracle/qkx_oracle.c) and the golden vectors are pinned to the
  * reference itself.  Single rank, P = (1,1,1,1), the MPI calls go to ref/mpi.h.
  *
@@ -223,6 +225,105 @@ double ref_cg_timed(const int L[4], double kappa, double mu, int twistSign, doub
   }
   store_vec(vout, x);
   return t1 - t0;
+}
+
+/* Gauge::calculatePlaquette (lib/lattice_util.cpp:923) of the links as given. */
+double ref_plaquette(const int L[4], const double* U) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  return u.calculatePlaquette();
+}
+
+/* qcd_projectSU33d (lib/blas.cpp:6) on the spatial links of U, in place. */
+void ref_project_su3(const int L[4], double* U) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  qcd_projectSU33d(u);
+  memcpy(U, &(u.M[0][0][0][0]), sizeof(double) * 72 * volume(L));
+}
+
+/* this->APE_smearing(U_tmp) (lib/lattice_util.cpp:948) with U_tmp = U_in and
+ * *this = U_out on entry; U_out receives *this afterwards. */
+void ref_ape_smear(const int L[4], const double* U_in, double* U_out, int nsmear, double alpha) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  li.NsmearAPE = nsmear;
+  li.alphaAPE = alpha;
+  Gauge tmp(&li), out(&li);
+  memcpy(&(tmp.M[0][0][0][0]), U_in, sizeof(double) * 72 * volume(L));
+  memcpy(&(out.M[0][0][0][0]), U_out, sizeof(double) * 72 * volume(L));
+  {
+    QuietStdout q;
+    out.APE_smearing(tmp, &li);
+  }
+  memcpy(U_out, &(out.M[0][0][0][0]), sizeof(double) * 72 * volume(L));
+}
+
+/* this->Gaussian_smearing(vec_tmp, gauge) (lib/lattice_util.cpp:1080) with
+ * vec_tmp = in and *this = out on entry; out receives *this afterwards. */
+void ref_gaussian_smear(const int L[4], const double* U, const double* in, double* out, int nsmear,
+                        double alpha) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  li.NsmearGauss = nsmear;
+  li.alphaGauss = alpha;
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  Vector vin(&li), vout(&li);
+  load_vec(vin, in);
+  load_vec(vout, out);
+  {
+    QuietStdout q;
+    vout.Gaussian_smearing(vin, u, &li);
+  }
+  store_vec(vout, out);
+}
+
+/* Propagator::absorbVector (lib/lattice_util.cpp:2073) into prop in place. */
+void ref_absorb_vector(const int L[4], const double* phi, int nu, int c2, double* prop) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Propagator p(&li);
+  memcpy(&(p.M[0][0][0][0][0]), prop, sizeof(double) * 288 * volume(L));
+  Vector v(&li);
+  load_vec(v, phi);
+  p.absorbVector(v, nu, c2);
+  memcpy(prop, &(p.M[0][0][0][0][0]), sizeof(double) * 288 * volume(L));
+}
+
+/* The propagator loop of bin/test_invert_prop.cpp:83-97: for each source
+ * spin-colour (mu, ic), a point source at site `src` is Gaussian-smeared with
+ * U_smear, the system M x = b is solved as tmDag + CG::operator() with the
+ * operator links U (boundary condition already applied), the solution is
+ * smeared and absorbed as column (mu, ic) of prop. */
+void ref_propagator(const int L[4], double kappa, double mu, int twistSign, double tol, int maxIter,
+                    const double* U, const double* U_smear, int nsmear, double alpha, long src, double* prop) {
+  LatticeInfo li = make_info(L, kappa, mu, twistSign, -1, tol, maxIter);
+  li.NsmearGauss = nsmear;
+  li.alphaGauss = alpha;
+  Gauge u(&li), us(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  memcpy(&(us.M[0][0][0][0]), U_smear, sizeof(double) * 72 * volume(L));
+  u.constGauge = true;
+  Vector vec_out(&li), vec_tmp(&li), vec_in(&li);
+  Propagator p(&li);
+  p.zero();
+  {
+    QuietStdout q;
+    CG cg(&li, u);
+    for (int sp = 0; sp < 4; sp++)
+      for (int ic = 0; ic < 3; ic++) {
+        vec_tmp.zero();
+        vec_out.zero();
+        vec_tmp.M[src][sp][ic].real() = 1.;
+        vec_out.Gaussian_smearing(vec_tmp, us, &li);
+        vec_in.tmDag(vec_out, u, &li);
+        vec_out.zero();
+        cg(vec_out, vec_in, &li);
+        vec_in.Gaussian_smearing(vec_out, us, &li);
+        p.absorbVector(vec_in, sp, ic);
+      }
+  }
+  memcpy(prop, &(p.M[0][0][0][0][0]), sizeof(double) * 288 * volume(L));
 }
 
 }  // extern "C"

@@ -12,6 +12,9 @@ reference's hot-path interface by name:
                              -- lib/blas_qkxTM.cpp, Vector::norm2
 * ``Lattice.invert``         -- the solve sequence tmDag + CG of bin/test_invert.cpp,
                                 with the B200 solvers (plain FP64 or even-odd mixed precision)
+* ``Lattice.calculatePlaquette / APE_smearing / Gaussian_smearing / absorbVector``
+                             -- Gauge / Vector / Propagator members (lib/lattice_util.cpp:923-1145, 2073)
+* ``Lattice.propagator``     -- the smeared-source propagator loop of bin/test_invert_prop.cpp
 
 Fields are numpy float64 arrays in the reference's host layouts: spinor
 ``[V, 4, 3, 2]`` (Vector::M) and gauge ``[V, 4, 3, 3, 2]`` (Gauge::M).
@@ -38,6 +41,7 @@ ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOGAUGE, ERR_NOT_CONVERGED, ERR_NAN, ERR_U
 
 LINKS_AS_GIVEN, LINKS_APPLY_BC = 0, 1
 NOALLOC_MAX_SITES = 11184810  # QKX_NOALLOC_MAX_SITES
+LINKS_OPERATOR, LINKS_SMEARING = 0, 1
 SOLVER_CG_FP64, SOLVER_CG_EO_MIXED = 0, 1
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
 
@@ -64,6 +68,9 @@ SYMBOLS = [
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
     "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
+    "qkx_plaquette", "qkx_plaquette_loaded", "qkx_project_su3", "qkx_ape_smear", "qkx_load_smearing_gauge",
+    "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
+    "qkx_propagator_dev",
 ]
 
 
@@ -154,6 +161,18 @@ def lib() -> C.CDLL:
         L.qkx_kernel_launches.argtypes = [_vp]
         L.qkx_kernel_launches.restype = C.c_longlong
         L.qkx_tune.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
+        L.qkx_plaquette.argtypes = [_vp, _vp, _dp]
+        L.qkx_plaquette_loaded.argtypes = [_vp, C.c_int, _dp]
+        L.qkx_project_su3.argtypes = [_vp, _vp]
+        L.qkx_ape_smear.argtypes = [_vp, _vp, _vp, C.c_int, C.c_double]
+        L.qkx_load_smearing_gauge.argtypes = [_vp, _vp]
+        L.qkx_gaussian_smear.argtypes = [_vp, C.c_int, C.POINTER(_vp), C.POINTER(_vp), C.c_int,
+                                         C.c_double]
+        L.qkx_gaussian_smear_dev.argtypes = L.qkx_gaussian_smear.argtypes
+        L.qkx_propagator_absorb.argtypes = [_vp, _vp, C.c_int, C.c_int, _vp]
+        L.qkx_propagator.argtypes = [_vp, C.POINTER(SolverParams), C.c_int, C.c_double,
+                                     C.POINTER(C.c_int), _vp, C.POINTER(SolveInfo)]
+        L.qkx_propagator_dev.argtypes = L.qkx_propagator.argtypes
         _lib = L
     return _lib
 
@@ -377,6 +396,83 @@ class Lattice:
         sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
         info = SolveInfo()
         check(lib().qkx_invert_dev(self.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
+        return info
+
+    # ------------------------------------------------------------ gauge-side stencils
+    def plaquette(self, U: np.ndarray | None = None, which: int = LINKS_OPERATOR) -> float:
+        """Gauge::calculatePlaquette of host links U, or of a field the context holds."""
+        r = C.c_double()
+        if U is not None:
+            check(lib().qkx_plaquette(self.ctx, _host(U).ctypes.data, C.byref(r)))
+        else:
+            check(lib().qkx_plaquette_loaded(self.ctx, which, C.byref(r)))
+        return r.value
+
+    calculatePlaquette = plaquette
+
+    def project_su3(self, U: np.ndarray) -> np.ndarray:
+        """qcd_projectSU33d on the spatial links of a copy of U."""
+        U = _host(U).copy()
+        check(lib().qkx_project_su3(self.ctx, U.ctypes.data))
+        return U
+
+    def APE_smearing(self, U_in: np.ndarray, nsmear: int = 20, alpha: float = 0.5,
+                     out: np.ndarray | None = None) -> np.ndarray | None:
+        """Gauge::APE_smearing of U_in; the result also becomes the smearing links.
+        Returns the smeared field (out, or a new array); nsmear == 0 leaves out as it was."""
+        out = np.zeros_like(_host(U_in)) if out is None else out
+        check(lib().qkx_ape_smear(self.ctx, _host(U_in).ctypes.data, out.ctypes.data, nsmear, alpha))
+        return out
+
+    def load_smearing_gauge(self, U: np.ndarray) -> None:
+        check(lib().qkx_load_smearing_gauge(self.ctx, _host(U).ctypes.data))
+
+    def Gaussian_smearing(self, psis: Sequence[np.ndarray], nsmear: int = 50, alpha: float = 4.0,
+                          out: Sequence[np.ndarray] | None = None) -> list:
+        """Vector::Gaussian_smearing of every field of psis with the smearing links."""
+        psis = [_host(p) for p in psis]
+        outs = [np.zeros_like(p) for p in psis] if out is None else list(out)
+        n = len(psis)
+        ip = (_vp * n)(*[p.ctypes.data for p in psis])
+        op = (_vp * n)(*[o.ctypes.data for o in outs])
+        check(lib().qkx_gaussian_smear(self.ctx, n, ip, op, nsmear, alpha))
+        return outs
+
+    def Gaussian_smearing_dev(self, src: Sequence[DeviceField], dst: Sequence[DeviceField],
+                              nsmear: int = 50, alpha: float = 4.0) -> None:
+        n = len(src)
+        ip = (_vp * n)(*[f.ptr for f in src])
+        op = (_vp * n)(*[f.ptr for f in dst])
+        check(lib().qkx_gaussian_smear_dev(self.ctx, n, ip, op, nsmear, alpha))
+
+    def absorbVector(self, prop: np.ndarray, phi: np.ndarray, nu: int, c2: int) -> None:
+        """Propagator::absorbVector: prop[x, mu, nu, c1, c2] = phi[x, mu, c1] (prop in place)."""
+        assert prop.dtype == np.float64 and prop.flags["C_CONTIGUOUS"] and prop.size == self.V * 288
+        check(lib().qkx_propagator_absorb(self.ctx, _host(phi).ctypes.data, nu, c2, prop.ctypes.data))
+
+    def propagator(self, x_src=(0, 0, 0, 0), nsmear: int = 50, alpha: float = 4.0,
+                   method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF, tol: float = 1e-10,
+                   maxIter: int = 10000, reliable_delta: float = 0.0, use_graphs: int = 1,
+                   out: np.ndarray | None = None):
+        """The smeared-source propagator [V, 4, 4, 3, 3, 2] at x_src; returns (prop, info)."""
+        prop = np.empty((self.V, 4, 4, 3, 3, 2)) if out is None else out
+        assert prop.dtype == np.float64 and prop.flags["C_CONTIGUOUS"] and prop.size == self.V * 288
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        info = SolveInfo()
+        rc = lib().qkx_propagator(self.ctx, C.byref(sp), nsmear, alpha, (C.c_int * 4)(*x_src),
+                                  prop.ctypes.data, C.byref(info))
+        check(rc)
+        return prop, info
+
+    def propagator_dev(self, prop_ptr: int, x_src=(0, 0, 0, 0), nsmear: int = 50, alpha: float = 4.0,
+                       method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF, tol: float = 1e-10,
+                       maxIter: int = 10000, reliable_delta: float = 0.0,
+                       use_graphs: int = 1) -> SolveInfo:
+        """The same into device memory at prop_ptr (V * 2304 bytes, host layout); asynchronous."""
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        info = SolveInfo()
+        check(lib().qkx_propagator_dev(self.ctx, C.byref(sp), nsmear, alpha, (C.c_int * 4)(*x_src),
+                                       prop_ptr, C.byref(info)))
         return info
 
     # ------------------------------------------------------------ profiling

@@ -358,7 +358,7 @@ int run_op(qkx_ctx* c, int op, const double2* in, double2* out) {
   }
 }
 
-static int upload_spinor(qkx_ctx* c, const double* host, double2* dev) {
+int upload_spinor(qkx_ctx* c, const double* host, double2* dev) {
   QKX_TRY(ensure_stage(c));
   QKX_CUDA(cudaMemcpyAsync(c->stage, host, sizeof(double2) * 12 * c->V, cudaMemcpyHostToDevice, c->st));
   k_spinor_aos_to_eo<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->stage, dev, c->geom);
@@ -367,7 +367,7 @@ static int upload_spinor(qkx_ctx* c, const double* host, double2* dev) {
   return QKX_OK;
 }
 
-static int download_spinor(qkx_ctx* c, const double2* dev, double* host) {
+int download_spinor(qkx_ctx* c, const double2* dev, double* host) {
   QKX_TRY(ensure_stage(c));
   k_spinor_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(dev, c->stage, c->geom);
   counted(c);
@@ -506,6 +506,7 @@ void qkx_destroy(qkx_ctx* c) {
   cudaFree(c->U12f);
   cudaFree(c->U12ha);
   cudaFree(c->U12hb);
+  cudaFree(c->Usm);
   cudaFree(c->stage);
   for (int i = 0; i < qkx_ctx::NW; i++) cudaFree(c->w[i]);
   cudaFree(c->part);

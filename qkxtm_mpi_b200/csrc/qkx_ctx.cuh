@@ -48,6 +48,8 @@ struct qkx_ctx {
   float4* U12f = nullptr;     // [2][4][3][Vh] FP32 12-real, SU(3)
   uint4* U12ha = nullptr;     // [2][4][Vh]  FP16 12-real complex 0..3
   uint2* U12hb = nullptr;     // [2][4][Vh]  FP16 12-real complex 4..5
+  double2* Usm = nullptr;     // [2][4][9][Vh] FP64 links of the Gaussian smearing (APE-smeared)
+  int have_smear = 0;
   double2* stage = nullptr;   // one host-layout spinor (V*12 double2)
   static constexpr int NW = 8;
   double2* w[NW] = {};        // FP64 full-lattice work fields
@@ -128,5 +130,13 @@ int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const dou
 void mixed_free(qkx_ctx* c);
 void mixed_invalidate(qkx_ctx* c);
 int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
+
+// lazy buffers and context-level helpers (api.cu)
+int ensure_stage(qkx_ctx* c);
+int ensure_links(qkx_ctx* c);
+int ensure_work(qkx_ctx* c);
+// host Vector::M layout <-> device even-odd FP64 field, through the staging buffer
+int upload_spinor(qkx_ctx* c, const double* host, double2* dev);
+int download_spinor(qkx_ctx* c, const double2* dev, double* host);
 
 }  // namespace qkx

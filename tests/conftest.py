@@ -42,3 +42,25 @@ def rel(a, b) -> float:
     b = np.asarray(b, dtype=np.float64)
     nb = np.linalg.norm(b.ravel())
     return float(np.linalg.norm((a - b).ravel()) / (nb if nb > 0 else 1.0))
+
+
+def site_index(L, x) -> int:
+    return int(x[0] + L[0] * (x[1] + L[1] * (x[2] + L[2] * x[3])))
+
+
+def oracle_propagator(O, L, U_op, U_smear, kappa, mu, nsmear, alpha, x_src, tol=1e-12, maxIter=2000):
+    """The propagator loop of the reference's bin/test_invert_prop.cpp:83-97 composed from
+    oracle pieces: point source -> Gaussian smearing -> tmDag -> CG -> smearing -> absorbVector."""
+    V = O.volume(L)
+    prop = np.zeros((V, 4, 4, 3, 3, 2))
+    for sp in range(4):
+        for ic in range(3):
+            b = O.spinor_point(L, x_src, sp, ic)
+            if nsmear > 0:
+                b = O.gaussian_smear(L, U_smear, b, nsmear, alpha)
+            rhs = O.apply("tm_dag", L, U_op, b, kappa, mu)
+            x, _, _ = O.cg(L, U_op, rhs, kappa, mu, tol=tol, maxIter=maxIter)
+            if nsmear > 0:
+                x = O.gaussian_smear(L, U_smear, x, nsmear, alpha)
+            O.absorb_vector(x, sp, ic, prop)
+    return prop

@@ -16,6 +16,11 @@ Fixtures:
                       lattice 4x4x4x8
   ref_cg.npz          CG::operator() solution probes and true residual,
                       lattices 4x4x4x8 and 8x8x8x16
+  ref_smear.npz       Gauge::calculatePlaquette, qcd_projectSU33d, Gauge::APE_smearing,
+                      Vector::Gaussian_smearing and the propagator loop of
+                      bin/test_invert_prop.cpp, lattice 4x4x4x8
+
+    python tests/golden/make_golden.py smear    (only ref_smear.npz)
 """
 from __future__ import annotations
 
@@ -58,10 +63,65 @@ def sample_sites(L, n=16):
     return np.unique(np.linspace(0, V - 1, n).astype(np.int64))
 
 
+def perturbed_links(L, U, scale, seed):
+    """U plus scale times unit normals (three Gaussian spinor fields fill the 72 reals of a site)."""
+    g = np.concatenate([O.spinor_gaussian(L, seed + k).reshape(-1, 24) for k in range(3)], axis=1)
+    return U + scale * g.reshape(U.shape)
+
+
+SMEAR = {"L": (4, 4, 4, 8), "seed_u": 51, "seed_psi": 52, "seed_pert": 53, "ape_n": 20, "ape_alpha": 0.5,
+         "gauss_n": 50, "gauss_alpha": 4.0, "prop_n": 5, "prop_alpha": 4.0, "prop_src": (1, 2, 3, 5),
+         "prop_tol": 1e-12}
+
+
+def make_smear():
+    c = SMEAR
+    L = c["L"]
+    U = O.gauge_random(L, EPS, c["seed_u"])
+    psi = O.spinor_gaussian(L, c["seed_psi"])
+    sites = sample_sites(L)
+    W = probes(L)
+    d = {k: np.array(v) for k, v in c.items()}
+    d["eps"], d["kappa"], d["mu"] = EPS, KAPPA, MU
+    d["sites"] = sites
+    d["in_checksum"] = np.concatenate([checksum(U), checksum(psi)])
+    Ubc = O.apply_bc(L, U, -1)
+    d["plaq"] = np.array([O.ref_plaquette(L, U)])
+    d["plaq_bc"] = np.array([O.ref_plaquette(L, Ubc)])
+    P = O.ref_project_su3(L, perturbed_links(L, U, 0.3, c["seed_pert"]))
+    d["proj:sites"] = P[sites]
+    d["proj:checksum"] = checksum(P)
+    for n in (1, 2):
+        A = O.ref_ape_smear(L, U, n, c["ape_alpha"])
+        d[f"ape{n}:sites"] = A[sites]
+        d[f"ape{n}:checksum"] = checksum(A)
+    A = O.ref_ape_smear(L, U, c["ape_n"], c["ape_alpha"])
+    d["ape:sites"] = A[sites]
+    d["ape:checksum"] = checksum(A)
+    d["ape:plaq"] = np.array([O.ref_plaquette(L, A)])
+    for n in (1, c["gauss_n"]):
+        g = O.ref_gaussian_smear(L, A, psi, n, c["gauss_alpha"])
+        d[f"gauss{n}:sites"] = g[sites]
+        d[f"gauss{n}:norm2"] = np.array([np.sum(g * g)])
+        d[f"gauss{n}:probe"] = np.array([np.sum(w * g) for w in W])
+    src = c["prop_src"]
+    s = src[0] + L[0] * (src[1] + L[1] * (src[2] + L[2] * src[3]))
+    prop = O.ref_propagator(L, Ubc, A, KAPPA, MU, c["prop_n"], c["prop_alpha"], src=s, tol=c["prop_tol"],
+                            maxIter=2000)
+    d["prop:sites"] = prop[sites]
+    d["prop:norm2"] = np.array([np.sum(prop * prop)])
+    d["prop:checksum"] = checksum(prop)
+    np.savez_compressed(os.path.join(HERE, "ref_smear.npz"), **d)
+    print("ref_smear.npz", os.path.getsize(os.path.join(HERE, "ref_smear.npz")), "bytes")
+
+
 def main():
     O.build(ref=True)
     if not O.ref_available():
         raise SystemExit("reference build missing (oracle/_ref/libqkxref.so)")
+    if sys.argv[1:] == ["smear"]:
+        make_smear()
+        return
 
     # --- small lattice, full outputs
     L = (4, 2, 2, 4)
@@ -123,6 +183,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "ref_cg.npz"), **d)
     for f in ("ref_ops_small.npz", "ref_ops_probe.npz", "ref_cg.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
+    make_smear()
 
 
 if __name__ == "__main__":
