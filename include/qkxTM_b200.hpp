@@ -157,6 +157,11 @@ class Vector {
   void tm_xx_chiral(Vector& psi, Gauge& u, LatticeInfo* li, PARITY parity);
   void tm_xxDagTm_xx_chiral(Vector& psi, Gauge& u, LatticeInfo* li, PARITY parity);
 
+  // lib/lattice_util.cpp:1080-1145: *this = nsmear Gaussian smearing steps of
+  // vec_tmp with the links of gauge (li->NsmearGauss, li->alphaGauss).  vec_tmp
+  // is left unchanged (the reference overwrites it); nsmear == 0 leaves *this.
+  void Gaussian_smearing(Vector& vec_tmp, Gauge& gauge, LatticeInfo* li);
+
  private:
   friend class Gauge;
   void site(int op, Vector& psi, LatticeInfo* li);
@@ -180,11 +185,11 @@ class Gauge {
 
   void zero() {
     std::fill(storage_.begin(), storage_.end(), Complex(0, 0));
-    dirty_ = true;
+    dirty_ = smear_dirty_ = true;
   }
   void copy(Gauge& src) {
     std::memcpy(M, src.M, sizeof(Complex) * 36 * lV4d);
-    dirty_ = true;
+    dirty_ = smear_dirty_ = true;
   }
   // lib/lattice_util.cpp:708-724: t-links on the last time slice change sign when boundaryT == -1
   void applyBoundaryCondition(LatticeInfo* li) {
@@ -193,13 +198,39 @@ class Gauge {
     for (long iv = lV4d - V3; iv < lV4d; iv++)
       for (int a = 0; a < 3; a++)
         for (int b = 0; b < 3; b++) M[iv][3][a][b] = -M[iv][3][a][b];
-    dirty_ = true;
+    dirty_ = smear_dirty_ = true;
   }
   // push M to the device now (needed after writing M directly once the field was used)
   void upload() {
     check(qkx_load_gauge(ctx_->c, reinterpret_cast<const double*>(storage_.data()), QKX_LINKS_AS_GIVEN));
     dirty_ = false;
+    smear_dirty_ = true;
   }
+
+  // lib/lattice_util.cpp:923-946, on the GPU
+  double calculatePlaquette() {
+    double r = 0;
+    check(qkx_plaquette_loaded(ctx(&info_), QKX_LINKS_OPERATOR, &r));
+    return r;
+  }
+  // lib/lattice_util.cpp:948-1078: *this = APE smearing of U_tmp (li->NsmearAPE,
+  // li->alphaAPE), spatial links projected to SU(3), t-links of U_tmp.  U_tmp is
+  // left unchanged (the reference overwrites it); nsmear == 0 leaves *this.
+  void APE_smearing(Gauge& U_tmp, LatticeInfo* li) {
+    if (li->NsmearAPE == 0) return;
+    check(qkx_ape_smear(ctx_->c, U_tmp.data(), data(), li->NsmearAPE, li->alphaAPE));
+    dirty_ = true;          // operator links are re-uploaded on next use
+    smear_dirty_ = false;   // the context's smearing links are this result
+  }
+  // the library context with M as its smearing links (for Gaussian smearing)
+  qkx_ctx* smear_ctx() {
+    if (smear_dirty_) {
+      check(qkx_load_smearing_gauge(ctx_->c, data()));
+      smear_dirty_ = false;
+    }
+    return ctx_->c;
+  }
+  double* data() { return reinterpret_cast<double*>(storage_.data()); }
   // the library context of this gauge field, with the parameters of li
   qkx_ctx* ctx(const LatticeInfo* li) {
     if (dirty_) upload();
@@ -213,6 +244,7 @@ class Gauge {
   std::unique_ptr<detail::Ctx> ctx_;
   std::vector<Complex> storage_;
   bool dirty_ = true;
+  bool smear_dirty_ = true;
 };
 
 // ---- Vector members that need a gauge field
@@ -323,6 +355,39 @@ inline void X_eq_aX_p_Y(Vector& x, double a, Vector& y) {
   check(qkx_spinor_download(c, dx.p, x.data()));
 }
 
+inline void Vector::Gaussian_smearing(Vector& vec_tmp, Gauge& gauge, LatticeInfo* li) {
+  if (li->NsmearGauss == 0) return;
+  const double* in[1] = {vec_tmp.data()};
+  double* out[1] = {data()};
+  check(qkx_gaussian_smear(gauge.smear_ctx(), 1, in, out, li->NsmearGauss, li->alphaGauss));
+}
+
+// qkxTM::Propagator (include/lattice_util.h:158-183), hot-path members.
+class Propagator {
+ public:
+  long size, size_total, lV4d;
+  Complex (*M)[4][4][3][3];
+
+  explicit Propagator(LatticeInfo* li) : info_(*li) {
+    lV4d = size = size_total = li->volume();
+    storage_.assign((size_t)lV4d * 144, Complex(0, 0));
+    M = reinterpret_cast<Complex(*)[4][4][3][3]>(storage_.data());
+  }
+  virtual ~Propagator() {}
+  void zero() { std::fill(storage_.begin(), storage_.end(), Complex(0, 0)); }
+  void copy(Propagator& src) { std::memcpy(M, src.M, sizeof(Complex) * 144 * lV4d); }
+  // lib/lattice_util.cpp:2073-2081: M[x][mu][nu][c1][c2] = phi.M[x][mu][c1],
+  // moved by the GPU's copy engines
+  void absorbVector(Vector& phi, int nu, int c2) {
+    check(qkx_propagator_absorb(detail::plain_ctx(info_), phi.data(), nu, c2, data()));
+  }
+  double* data() { return reinterpret_cast<double*>(storage_.data()); }
+
+ private:
+  LatticeInfo info_;
+  std::vector<Complex> storage_;
+};
+
 // ---- class CG (include/solvers.h:3-22, lib/solvers.cpp)
 class CG {
  public:
@@ -362,6 +427,28 @@ class CG {
     sp.mu = nullptr;
     qkx_solve_info info;
     check(qkx_invert(u_.ctx(param), &sp, (int)bp.size(), bp.data(), xp.data(), &info));
+    return info;
+  }
+
+  // B200 smeared-source propagator (no reference counterpart; replaces the
+  // loop of bin/test_invert_prop.cpp:83-97): 12 point sources at
+  // param->x_src, Gaussian smearing with the links of smear_gauge
+  // (param->NsmearGauss, param->alphaGauss) at source and sink, one batched
+  // solve, the columns assembled into prop.
+  qkx_solve_info propagator(Propagator& prop, Gauge& smear_gauge, LatticeInfo* param,
+                            int method = QKX_SOLVER_CG_EO_MIXED, int precision = QKX_PREC_HALF, double tol = 1e-10) {
+    qkx_ctx* c = u_.ctx(param);
+    if (param->NsmearGauss > 0) check(qkx_load_smearing_gauge(c, smear_gauge.data()));
+    qkx_solver_params sp;
+    sp.method = method;
+    sp.sloppy_precision = precision;
+    sp.tol = tol;
+    sp.maxIter = 100000;
+    sp.reliable_delta = 0.0;
+    sp.use_graphs = 1;
+    sp.mu = nullptr;
+    qkx_solve_info info;
+    check(qkx_propagator(c, &sp, param->NsmearGauss, param->alphaGauss, param->x_src, prop.data(), &info));
     return info;
   }
 

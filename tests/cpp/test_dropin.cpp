@@ -1,6 +1,7 @@
 // test_dropin.cpp -- the reference's driver flow (bin/test_applyTM.cpp,
-// bin/test_invert.cpp) written against include/qkxTM_b200.hpp, checked
-// against the CPU oracle.  Built and run by tests/test_gpu_dropin.py.
+// bin/test_invert.cpp, bin/test_invert_prop.cpp) written against
+// include/qkxTM_b200.hpp, checked against the CPU oracle.  Built and run by
+// tests/test_gpu_dropin.py.
 #include <cmath>
 #include <cstdio>
 
@@ -102,6 +103,68 @@ int main() {
     fails++;
   } catch (const Error& err) {
     printf("wrong parity  -> Error %d\n", err.code);
+  }
+
+  // bin/test_invert_prop.cpp: plaquettes, APE smearing, the smeared-source
+  // propagator loop with the drop-in classes, and the batched B200 call
+  {
+    LatticeInfo li;
+    li.L[0] = li.L[1] = li.L[2] = 4;
+    li.L[3] = 8;
+    li.kappa = 0.16;
+    li.mu = 0.01;
+    li.tol = 1e-12;
+    li.maxIter = 5000;
+    li.NsmearAPE = 20;
+    li.alphaAPE = 0.5;
+    li.NsmearGauss = 5;
+    li.alphaGauss = 4.0;
+    li.x_src[0] = 1;
+    li.x_src[1] = 2;
+    li.x_src[2] = 3;
+    li.x_src[3] = 5;
+    Gauge* g = new Gauge(&li);
+    Gauge* g_tmp = new Gauge(&li);
+    Gauge* g_ape = new Gauge(&li);
+    const long Vs = g->lV4d;
+    orc_gauge_random(li.L, 0.3, 51, g->data());
+    g_tmp->copy(*g);
+    double plaq = g->calculatePlaquette();
+    double pref = orc_plaquette_ref(li.L, g->data());
+    printf("plaquette     %.12f (oracle %.12f)\n", plaq, pref);
+    fails += std::fabs(plaq - pref) > 1e-13;
+    g_ape->APE_smearing(*g_tmp, &li);
+    std::vector<double> ape(72 * Vs);
+    orc_ape_smear(li.L, g->data(), ape.data(), li.NsmearAPE, li.alphaAPE);
+    e = rel(g_ape->data(), ape.data(), 72 * Vs);
+    double pa = g_ape->calculatePlaquette();
+    printf("APE smearing  rel err %.2e, smeared plaquette %.12f\n", e, pa);
+    fails += e > 1e-10 || std::fabs(pa - orc_plaquette_ref(li.L, ape.data())) > 1e-12;
+    g->applyBoundaryCondition(&li);
+
+    Vector v_out(&li), v_tmp(&li), v_in(&li);
+    Propagator prop(&li), prop2(&li);
+    CG cgp(&li, *g);
+    const long src = li.x_src[0] + 4 * (li.x_src[1] + 4 * (li.x_src[2] + 4 * li.x_src[3]));
+    for (int mu = 0; mu < 4; mu++)
+      for (int ic = 0; ic < 3; ic++) {
+        v_tmp.zero();
+        v_out.zero();
+        v_tmp.M[src][mu][ic] = 1.0;
+        v_out.Gaussian_smearing(v_tmp, *g_ape, &li);
+        v_in.tmDag(v_out, *g, &li);
+        v_out.zero();
+        cgp(v_out, v_in, &li);
+        v_in.Gaussian_smearing(v_out, *g_ape, &li);
+        prop.absorbVector(v_in, mu, ic);
+      }
+    qkx_solve_info pi = cgp.propagator(prop2, *g_ape, &li, QKX_SOLVER_CG_EO_MIXED, QKX_PREC_HALF, 1e-12);
+    e = rel(prop2.data(), prop.data(), 288 * Vs);
+    printf("propagator    batched vs loop rel err %.2e (true residual %.2e)\n", e, pi.true_residual);
+    fails += e > 1e-8;
+    delete g_ape;
+    delete g_tmp;
+    delete g;
   }
 
   delete vec_out;
