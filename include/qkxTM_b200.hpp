@@ -425,6 +425,7 @@ class CG {
     sp.reliable_delta = 0.0;
     sp.use_graphs = 1;
     sp.mu = nullptr;
+    sp.preconditioner = nullptr;
     qkx_solve_info info;
     check(qkx_invert(u_.ctx(param), &sp, (int)bp.size(), bp.data(), xp.data(), &info));
     return info;
@@ -447,6 +448,7 @@ class CG {
     sp.reliable_delta = 0.0;
     sp.use_graphs = 1;
     sp.mu = nullptr;
+    sp.preconditioner = nullptr;
     qkx_solve_info info;
     check(qkx_propagator(c, &sp, param->NsmearGauss, param->alphaGauss, param->x_src, prop.data(), &info));
     return info;

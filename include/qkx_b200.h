@@ -198,6 +198,7 @@ typedef struct qkx_solve_info {
   double true_residual;    /* max over RHS of ||b - M x|| / ||b||, recomputed in FP64 */
   double normal_residual;  /* max over RHS of the final CG residual ||r|| / ||in|| */
   double seconds;          /* device time of the solve (CUDA events) */
+  int fallbacks;           /* right-hand sides that QKX_SOLVER_GCR_PTC handed to the plain solver */
 } qkx_solve_info;
 
 /* CG::operator()(out, in, param) (lib/solvers.cpp:16-81), FP64, full lattice:
@@ -211,6 +212,9 @@ QKX_API int qkx_cg_dev(qkx_ctx* ctx, const double* in_dev, double* x_dev, qkx_so
 /* Solver methods for qkx_invert. */
 #define QKX_SOLVER_CG_FP64 0        /* plain FP64 CG on M^+M, full lattice (the reference's method) */
 #define QKX_SOLVER_CG_EO_MIXED 1    /* even-odd Schur CG, sloppy spinors/links, FP64 reliable updates */
+#define QKX_SOLVER_GCR_PTC 2        /* flexible GCR(16) on M in FP32 with the learned preconditioner
+                                       (sp->preconditioner; NULL = none), FP64 defect correction,
+                                       and CG_EO_MIXED as the fallback */
 
 #define QKX_PREC_DOUBLE 0
 #define QKX_PREC_SINGLE 1
@@ -226,6 +230,7 @@ typedef struct qkx_solver_params {
   int use_graphs;          /* replay the inner iteration from a CUDA graph */
   const double* mu;        /* NULL, or nrhs twisted masses (one per right-hand side, the
                               multi-mass solve of CG_EO_MIXED); NULL = the context's mu */
+  const struct qkx_ptc* preconditioner;  /* QKX_SOLVER_GCR_PTC: the trained network, or NULL */
 } qkx_solver_params;
 
 /* Solve M x_i = b_i for nrhs right-hand sides (host buffers, Vector::M layout),
@@ -310,6 +315,61 @@ QKX_API int qkx_propagator(qkx_ctx* ctx, const qkx_solver_params* sp, int nsmear
 /* The same with the propagator written to device memory (V*2304 bytes, host layout). */
 QKX_API int qkx_propagator_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nsmear, double alpha,
                                const int x_src[4], double* prop_dev, qkx_solve_info* info);
+
+/* ---------------------------------------------------------------- learned preconditioner
+ * No reference counterpart.  A linear, gauge-covariant parallel-transport
+ * convolution network N approximating M^-1: layer l maps channels[l] to
+ * channels[l+1] colour vectors per site,
+ *   out(x)[c] = sum_{p=0..8} sum_c' W[p][c][c'] (T_p in)(x)[c'],
+ * T_0 = 1, T_{1+2mu} a(x) = U_mu(x) a(x+mu), T_{2+2mu} a(x) = U_mu(x-mu)^+ a(x-mu),
+ * with the context's links (boundary sign included).  channels[0] =
+ * channels[nlayers] = 4 (the spins), so N maps a spinor to a spinor.  Weights
+ * are complex, [9][channels[l+1]][channels[l]] per layer, layers concatenated;
+ * the kernels use BF16 copies with FP32 arithmetic.  Widths are 4, 8 or 16. */
+typedef struct qkx_ptc qkx_ptc;
+#define QKX_PTC_MAX_LAYERS 8
+
+typedef struct qkx_ptc_params {
+  int nlayers;                               /* 1..QKX_PTC_MAX_LAYERS */
+  int channels[QKX_PTC_MAX_LAYERS + 1];      /* widths, 4/8/16, first and last 4 */
+  unsigned long long seed;                   /* random initial weights */
+  double init_scale;                         /* std of the initial hop-path weights (identity path starts
+                                                as the identity, so N starts close to 1) */
+} qkx_ptc_params;
+
+typedef struct qkx_ptc_train_params {
+  int n_solves;            /* (residual, error) pairs from as many mixed-precision CG solves of
+                              Gaussian sources, r = b and e = M^-1 b, plus as many pairs r = M v,
+                              e = v for Gaussian v (the short-distance part of M^-1) */
+  int steps;               /* Adam steps, one pair each, pairs in a seeded shuffled order */
+  double lr;               /* peak learning rate (cosine decay to lr/20) */
+  double solve_tol;        /* true-residual tolerance of the data solves */
+  unsigned long long seed; /* sources and pair order */
+} qkx_ptc_train_params;
+
+typedef struct qkx_ptc_train_info {
+  double loss_initial;     /* mean |N(r) - e|^2 / |e|^2 over up to 4 pairs of each kind, before */
+  double loss_final;       /* the same after training */
+  double seconds_data;     /* device time of the data solves */
+  double seconds_train;    /* device time of the training steps */
+  int steps;
+} qkx_ptc_train_info;
+
+QKX_API int qkx_ptc_create(qkx_ctx* ctx, const qkx_ptc_params* p, qkx_ptc** out);
+QKX_API void qkx_ptc_destroy(qkx_ptc* net);
+/* number of complex weights */
+QKX_API long qkx_ptc_num_weights(const qkx_ptc* net);
+/* weights as [n][2] doubles: which = 0 the FP32 master copy, 1 the BF16 copy the kernels use */
+QKX_API int qkx_ptc_get_weights(const qkx_ptc* net, int which, double* w);
+QKX_API int qkx_ptc_set_weights(qkx_ptc* net, const double* w);
+/* out = N(in), host spinors (Vector::M layout) */
+QKX_API int qkx_ptc_apply(qkx_ptc* net, const double* in_host, double* out_host);
+/* loss |N(r) - e|^2 / |e|^2 on one pair and its gradient dL/dW^* ([n][2] doubles, may be NULL),
+ * computed by the training kernels with the BF16 weights */
+QKX_API int qkx_ptc_loss_grad(qkx_ptc* net, const double* r_host, const double* e_host, double* loss,
+                              double* grad);
+/* make the training pairs with the context's solver and train with Adam */
+QKX_API int qkx_ptc_train(qkx_ptc* net, const qkx_ptc_train_params* tp, qkx_ptc_train_info* info);
 
 /* ---------------------------------------------------------------- memory helpers */
 /* Page-locked host memory for fast transfers (cudaHostAlloc); NULL on failure. */

@@ -95,6 +95,11 @@ def lib():
         L.orc_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
         L.orc_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
         L.orc_absorb_vector.argtypes = [C.c_long, _dp, C.c_int, C.c_int, _dp]
+        L.orc_ptc_nweights.argtypes = [C.c_int, _ip]
+        L.orc_ptc_nweights.restype = C.c_long
+        L.orc_ptc_forward.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
+        L.orc_ptc_loss_grad.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
+        L.orc_ptc_loss_grad.restype = C.c_double
     return _lib
 
 
@@ -326,3 +331,28 @@ def ref_propagator(L, U, U_smear, kappa, mu, nsmear, alpha, src=0, twistSign=1, 
     ref().ref_propagator(_L(L), kappa, mu, twistSign, tol, maxIter, _ptr(np.ascontiguousarray(U)),
                          _ptr(np.ascontiguousarray(U_smear)), nsmear, alpha, src, _ptr(prop))
     return prop
+
+
+# ---------------------------------------------------------------- learned preconditioner (PTC network)
+def ptc_nweights(ch) -> int:
+    """Complex weights of a PTC network with channel widths ch (9 paths per layer)."""
+    return int(lib().orc_ptc_nweights(len(ch) - 1, (C.c_int * len(ch))(*ch)))
+
+
+def ptc_forward(L, U, ch, W, x) -> np.ndarray:
+    """N(x) for x [V, ch[0], 3, 2]; W complex weights as float64 [nweights, 2]."""
+    V = volume(L)
+    out = np.empty((V, ch[-1], 3, 2))
+    lib().orc_ptc_forward(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1, (C.c_int * len(ch))(*ch),
+                          _ptr(np.ascontiguousarray(W)), _ptr(np.ascontiguousarray(x)), _ptr(out), None)
+    return out
+
+
+def ptc_loss_grad(L, U, ch, W, r, e, grad=True):
+    """(|N(r) - e|^2 / |e|^2, dL/dW^* as [nweights, 2] or None)."""
+    g = np.zeros_like(W) if grad else None
+    loss = lib().orc_ptc_loss_grad(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1,
+                                   (C.c_int * len(ch))(*ch), _ptr(np.ascontiguousarray(W)),
+                                   _ptr(np.ascontiguousarray(r)), _ptr(np.ascontiguousarray(e)),
+                                   _ptr(g) if grad else None)
+    return loss, g

@@ -87,6 +87,15 @@ void orc_gaussian_smear(const int L[4], const double* U, const double* in, doubl
                         double alpha);
 void orc_absorb_vector(long V, const double* phi, int nu, int c2, double* prop);
 
+/* learned preconditioner (qkx_oracle_ptc.c; no reference counterpart): a linear
+ * parallel-transport convolution network with nlayers layers of channel widths
+ * ch[0..nlayers]; weights [9][ch[l+1]][ch[l]] complex per layer, concatenated. */
+long orc_ptc_nweights(int nlayers, const int* ch);
+void orc_ptc_forward(const int L[4], const double* U, int nlayers, const int* ch, const double* W,
+                     const double* in, double* out, double* acts);
+double orc_ptc_loss_grad(const int L[4], const double* U, int nlayers, const int* ch, const double* W,
+                         const double* r, const double* e, double* grad);
+
 #ifdef __cplusplus
 }
 #endif

@@ -42,7 +42,7 @@ ERR_INVALID, ERR_CUDA, ERR_NOMEM, ERR_NOGAUGE, ERR_NOT_CONVERGED, ERR_NAN, ERR_U
 LINKS_AS_GIVEN, LINKS_APPLY_BC = 0, 1
 NOALLOC_MAX_SITES = 11184810  # QKX_NOALLOC_MAX_SITES
 LINKS_OPERATOR, LINKS_SMEARING = 0, 1
-SOLVER_CG_FP64, SOLVER_CG_EO_MIXED = 0, 1
+SOLVER_CG_FP64, SOLVER_CG_EO_MIXED, SOLVER_GCR_PTC = 0, 1, 2
 PREC_DOUBLE, PREC_SINGLE, PREC_HALF = 0, 1, 2
 
 # operator ids of enum qkx_op
@@ -70,7 +70,8 @@ SYMBOLS = [
     "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
     "qkx_plaquette", "qkx_plaquette_loaded", "qkx_project_su3", "qkx_ape_smear", "qkx_load_smearing_gauge",
     "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
-    "qkx_propagator_dev",
+    "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
+    "qkx_ptc_set_weights", "qkx_ptc_apply", "qkx_ptc_loss_grad", "qkx_ptc_train",
 ]
 
 
@@ -89,13 +90,34 @@ class Params(C.Structure):
 class SolverParams(C.Structure):
     _fields_ = [("method", C.c_int), ("sloppy_precision", C.c_int), ("tol", C.c_double),
                 ("maxIter", C.c_int), ("reliable_delta", C.c_double), ("use_graphs", C.c_int),
-                ("mu", C.POINTER(C.c_double))]
+                ("mu", C.POINTER(C.c_double)), ("preconditioner", C.c_void_p)]
+
+
+PTC_MAX_LAYERS = 8
+
+
+class PtcParams(C.Structure):
+    _fields_ = [("nlayers", C.c_int), ("channels", C.c_int * (PTC_MAX_LAYERS + 1)), ("seed", C.c_ulonglong),
+                ("init_scale", C.c_double)]
+
+
+class PtcTrainParams(C.Structure):
+    _fields_ = [("n_solves", C.c_int), ("steps", C.c_int), ("lr", C.c_double), ("solve_tol", C.c_double),
+                ("seed", C.c_ulonglong)]
+
+
+class PtcTrainInfo(C.Structure):
+    _fields_ = [("loss_initial", C.c_double), ("loss_final", C.c_double), ("seconds_data", C.c_double),
+                ("seconds_train", C.c_double), ("steps", C.c_int)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
 
 
 class SolveInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("reliable_updates", C.c_int), ("converged", C.c_int),
                 ("restarts", C.c_int), ("true_residual", C.c_double),
-                ("normal_residual", C.c_double), ("seconds", C.c_double)]
+                ("normal_residual", C.c_double), ("seconds", C.c_double), ("fallbacks", C.c_int)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -173,6 +195,16 @@ def lib() -> C.CDLL:
         L.qkx_propagator.argtypes = [_vp, C.POINTER(SolverParams), C.c_int, C.c_double,
                                      C.POINTER(C.c_int), _vp, C.POINTER(SolveInfo)]
         L.qkx_propagator_dev.argtypes = L.qkx_propagator.argtypes
+        L.qkx_ptc_create.argtypes = [_vp, C.POINTER(PtcParams), C.POINTER(_vp)]
+        L.qkx_ptc_destroy.argtypes = [_vp]
+        L.qkx_ptc_destroy.restype = None
+        L.qkx_ptc_num_weights.argtypes = [_vp]
+        L.qkx_ptc_num_weights.restype = C.c_long
+        L.qkx_ptc_get_weights.argtypes = [_vp, C.c_int, _vp]
+        L.qkx_ptc_set_weights.argtypes = [_vp, _vp]
+        L.qkx_ptc_apply.argtypes = [_vp, _vp, _vp]
+        L.qkx_ptc_loss_grad.argtypes = [_vp, _vp, _vp, _dp, _vp]
+        L.qkx_ptc_train.argtypes = [_vp, C.POINTER(PtcTrainParams), C.POINTER(PtcTrainInfo)]
         _lib = L
     return _lib
 
@@ -366,7 +398,7 @@ class Lattice:
     def invert(self, bs: Sequence[np.ndarray], method: int = SOLVER_CG_EO_MIXED,
                precision: int = PREC_HALF, tol: float = 1e-10, maxIter: int = 10000,
                reliable_delta: float = 0.0, use_graphs: int = 1, strict: bool = True,
-               out: Sequence[np.ndarray] | None = None):
+               out: Sequence[np.ndarray] | None = None, preconditioner: "Ptc | None" = None):
         """Solve M x_i = b_i to ||b - M x|| / ||b|| <= tol (FP64 true residual).
         `out` may supply the solution arrays (e.g. page-locked buffers)."""
         bs = [_host(b) for b in bs]
@@ -379,7 +411,8 @@ class Lattice:
         n = len(bs)
         bp = (_vp * n)(*[b.ctypes.data for b in bs])
         xp = (_vp * n)(*[x.ctypes.data for x in xs])
-        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs, None,
+                          preconditioner.ptr if preconditioner is not None else None)
         info = SolveInfo()
         rc = lib().qkx_invert(self.ctx, C.byref(sp), n, bp, xp, C.byref(info))
         if rc != OK and (strict or rc != ERR_NOT_CONVERGED):
@@ -389,11 +422,12 @@ class Lattice:
     def invert_dev(self, bs: Sequence[DeviceField], xs: Sequence[DeviceField],
                    method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF,
                    tol: float = 1e-10, maxIter: int = 10000, reliable_delta: float = 0.0,
-                   use_graphs: int = 1) -> SolveInfo:
+                   use_graphs: int = 1, preconditioner: "Ptc | None" = None) -> SolveInfo:
         n = len(bs)
         bp = (_vp * n)(*[b.ptr for b in bs])
         xp = (_vp * n)(*[x.ptr for x in xs])
-        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs)
+        sp = SolverParams(method, precision, tol, maxIter, reliable_delta, use_graphs, None,
+                          preconditioner.ptr if preconditioner is not None else None)
         info = SolveInfo()
         check(lib().qkx_invert_dev(self.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
         return info
@@ -501,6 +535,63 @@ class Lattice:
 
     def stream(self) -> int:
         return int(lib().qkx_stream(self.ctx) or 0)
+
+
+class Ptc:
+    """The learned preconditioner: a linear gauge-covariant parallel-transport convolution
+    network on the lattice's links (no reference counterpart).  channels are the widths per
+    colour, first and last 4 (the spins)."""
+
+    def __init__(self, lat: Lattice, channels=(4, 16, 16, 16, 4), seed: int = 1, init_scale: float = 0.1):
+        self.lat = lat
+        self.channels = tuple(channels)
+        nl = len(channels) - 1
+        p = PtcParams(nl, (C.c_int * (PTC_MAX_LAYERS + 1))(*channels), seed, init_scale)
+        self.ptr = _vp()
+        check(lib().qkx_ptc_create(lat.ctx, C.byref(p), C.byref(self.ptr)))
+        self.nw = int(lib().qkx_ptc_num_weights(self.ptr))
+
+    def close(self):
+        if getattr(self, "ptr", None) and self.ptr.value:
+            lib().qkx_ptc_destroy(self.ptr)
+            self.ptr = _vp()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def weights(self, which: int = 0) -> np.ndarray:
+        """[nweights, 2]: which = 0 the FP32 master weights, 1 the BF16 weights the kernels use."""
+        w = np.empty((self.nw, 2))
+        check(lib().qkx_ptc_get_weights(self.ptr, which, w.ctypes.data))
+        return w
+
+    def set_weights(self, w: np.ndarray) -> None:
+        w = _host(w)
+        assert w.size == 2 * self.nw
+        check(lib().qkx_ptc_set_weights(self.ptr, w.ctypes.data))
+
+    def apply(self, psi: np.ndarray) -> np.ndarray:
+        out = np.empty((self.lat.V, 4, 3, 2))
+        check(lib().qkx_ptc_apply(self.ptr, _host(psi).ctypes.data, out.ctypes.data))
+        return out
+
+    def loss_grad(self, r: np.ndarray, e: np.ndarray, grad: bool = True):
+        """(|N(r) - e|^2 / |e|^2, dL/dW^* as [nweights, 2] or None)."""
+        loss = C.c_double()
+        g = np.empty((self.nw, 2)) if grad else None
+        check(lib().qkx_ptc_loss_grad(self.ptr, _host(r).ctypes.data, _host(e).ctypes.data, C.byref(loss),
+                                      g.ctypes.data if grad else None))
+        return loss.value, g
+
+    def train(self, n_solves: int = 64, steps: int = 2000, lr: float = 2e-3, solve_tol: float = 1e-6,
+              seed: int = 7) -> dict:
+        tp = PtcTrainParams(n_solves, steps, lr, solve_tol, seed)
+        info = PtcTrainInfo()
+        check(lib().qkx_ptc_train(self.ptr, C.byref(tp), C.byref(info)))
+        return info.as_dict()
 
 
 def pinned_array(shape) -> np.ndarray:

@@ -871,6 +871,7 @@ int qkx_invert_dev(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
   double2* const* x = (double2* const*)x_dev;
   if (sp->method == QKX_SOLVER_CG_FP64) return invert_cg_fp64(c, sp, nrhs, b, x, info);
   if (sp->method == QKX_SOLVER_CG_EO_MIXED) return invert_eo_mixed(c, sp, nrhs, b, x, info);
+  if (sp->method == QKX_SOLVER_GCR_PTC) return invert_gcr_ptc(c, sp, nrhs, b, x, info);
   return invalid("solver method");
 }
 

@@ -128,6 +128,9 @@ inline SpinorF64 H64(const double2* base, int parity, int Vh) {
 int invert_eo_mixed(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
                     double2* const* x, qkx_solve_info* info);
 void mixed_free(qkx_ctx* c);
+// flexible GCR with the learned preconditioner (ptc.cu)
+int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b, double2* const* x,
+                   qkx_solve_info* info);
 void mixed_invalidate(qkx_ctx* c);
 int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
 

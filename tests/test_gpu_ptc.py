@@ -1,0 +1,115 @@
+"""GPU tests of the learned preconditioner (no reference counterpart): the forward
+and backward kernels against the CPU oracle at the same BF16-rounded weights,
+training on the library's own solves, and the flexible GCR solver that uses it
+(true residual checked in FP64 by the oracle, gain over no preconditioner, and
+the plain-solver fallback).
+
+Tolerances: the kernels compute in FP32 (BF16 weights, FP32 activations,
+FP32 tile sums, FP64 across tiles), the oracle in FP64 at the same weights:
+forward 1e-5 relative, loss 1e-5, gradient 1e-4 (norm-relative)."""
+import numpy as np
+import pytest
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+L = (4, 4, 4, 8)
+KAPPA, MU = 0.16, 0.01
+CH = (4, 16, 16, 16, 4)
+
+
+@pytest.fixture(scope="module")
+def setup(qkx, oracle):
+    U = oracle.apply_bc(L, oracle.gauge_random(L, 0.3, 2024), -1)
+    lat = qkx.Lattice(qkx.LatticeInfo(L=L, kappa=KAPPA, mu=MU))
+    lat.load_gauge(U, qkx.LINKS_AS_GIVEN)
+    yield lat, U
+    lat.close()
+
+
+@pytest.mark.parametrize("ch", [CH, (4, 8, 4), (4, 16, 8, 4)])
+def test_forward_matches_oracle(qkx, oracle, setup, ch):
+    lat, U = setup
+    net = qkx.Ptc(lat, ch, seed=11, init_scale=0.3)
+    W = net.weights(1)
+    for seed in (1, 2):
+        r = oracle.spinor_gaussian(L, seed)
+        got = net.apply(r)
+        exp = oracle.ptc_forward(L, U, list(ch), W, r)
+        assert rel(got, exp) < 1e-5, (ch, rel(got, exp))
+    net.close()
+
+
+def test_identity_at_zero_init(qkx, oracle, setup):
+    lat, _ = setup
+    net = qkx.Ptc(lat, CH, seed=1, init_scale=0.0)
+    r = oracle.spinor_gaussian(L, 3)
+    assert rel(net.apply(r), r) < 1e-7
+    net.close()
+
+
+def test_loss_and_gradient_match_oracle(qkx, oracle, setup):
+    lat, U = setup
+    for ch in (CH, (4, 8, 4)):
+        net = qkx.Ptc(lat, ch, seed=5, init_scale=0.3)
+        W = net.weights(1)
+        r = oracle.spinor_gaussian(L, 4)
+        e = oracle.spinor_gaussian(L, 5)
+        loss, g = net.loss_grad(r, e)
+        lo, go = oracle.ptc_loss_grad(L, U, list(ch), W, r, e)
+        assert abs(loss - lo) < 1e-5 * lo
+        assert rel(g, go) < 1e-4, (ch, rel(g, go))
+        # fixed-order reductions: the same gradient twice
+        loss2, g2 = net.loss_grad(r, e)
+        assert loss2 == loss and np.array_equal(g, g2)
+        net.close()
+
+
+@pytest.fixture(scope="module")
+def trained(qkx, setup):
+    lat, _ = setup
+    net = qkx.Ptc(lat, CH, seed=3, init_scale=0.05)
+    info = net.train(n_solves=16, steps=400, lr=3e-3, solve_tol=1e-7, seed=9)
+    yield net, info
+    net.close()
+
+
+def test_training_reduces_loss(trained):
+    _, info = trained
+    assert info["steps"] == 400
+    assert info["loss_final"] < 0.5 * info["loss_initial"], info
+
+
+def test_gcr_with_learned_preconditioner(qkx, oracle, setup, trained):
+    lat, U = setup
+    net, _ = trained
+    bs = [oracle.spinor_gaussian(L, 40 + k) for k in range(3)]
+    xs, info = lat.invert(bs, method=qkx.SOLVER_GCR_PTC, tol=1e-10, preconditioner=net)
+    assert info.converged == 1 and info.fallbacks == 0
+    for b, x in zip(bs, xs):
+        r = b - oracle.apply("tm", L, U, x, KAPPA, MU)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-10
+    _, plain = lat.invert(bs, method=qkx.SOLVER_GCR_PTC, tol=1e-10, preconditioner=None)
+    assert plain.converged == 1
+    # the trained network cuts the Krylov iterations
+    assert info.iterations < 0.7 * plain.iterations, (info.iterations, plain.iterations)
+
+
+def test_gcr_fallback_to_plain_solver(qkx, oracle, setup):
+    lat, U = setup
+    b = oracle.spinor_gaussian(L, 77)
+    (x,), info = lat.invert([b], method=qkx.SOLVER_GCR_PTC, tol=1e-10, maxIter=2, preconditioner=None)
+    assert info.fallbacks == 1 and info.converged == 1
+    r = b - oracle.apply("tm", L, U, x, KAPPA, MU)
+    assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-10
+
+
+def test_ptc_argument_checks(qkx, setup):
+    lat, _ = setup
+    with pytest.raises(qkx.QkxError) as e:
+        qkx.Ptc(lat, (4, 12, 4))
+    assert e.value.code == qkx.ERR_INVALID
+    with pytest.raises(qkx.QkxError) as e:
+        qkx.Ptc(lat, (8, 16, 4))
+    assert e.value.code == qkx.ERR_INVALID
