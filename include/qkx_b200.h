@@ -335,6 +335,10 @@ typedef struct qkx_ptc_params {
   unsigned long long seed;                   /* random initial weights */
   double init_scale;                         /* std of the initial hop-path weights (identity path starts
                                                 as the identity, so N starts close to 1) */
+  int tensor_cores;                          /* 1: the 16 -> 16 layers of qkx_ptc_apply and of the solver
+                                                run on the tensor cores (tcgen05, BF16 activations and
+                                                weights, FP32 accumulation); training always uses the
+                                                FP32-activation kernels */
 } qkx_ptc_params;
 
 typedef struct qkx_ptc_train_params {

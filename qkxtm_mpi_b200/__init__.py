@@ -98,7 +98,7 @@ PTC_MAX_LAYERS = 8
 
 class PtcParams(C.Structure):
     _fields_ = [("nlayers", C.c_int), ("channels", C.c_int * (PTC_MAX_LAYERS + 1)), ("seed", C.c_ulonglong),
-                ("init_scale", C.c_double)]
+                ("init_scale", C.c_double), ("tensor_cores", C.c_int)]
 
 
 class PtcTrainParams(C.Structure):
@@ -542,11 +542,12 @@ class Ptc:
     network on the lattice's links (no reference counterpart).  channels are the widths per
     colour, first and last 4 (the spins)."""
 
-    def __init__(self, lat: Lattice, channels=(4, 16, 16, 16, 4), seed: int = 1, init_scale: float = 0.1):
+    def __init__(self, lat: Lattice, channels=(4, 16, 16, 16, 4), seed: int = 1, init_scale: float = 0.1,
+                 tensor_cores: bool = True):
         self.lat = lat
         self.channels = tuple(channels)
         nl = len(channels) - 1
-        p = PtcParams(nl, (C.c_int * (PTC_MAX_LAYERS + 1))(*channels), seed, init_scale)
+        p = PtcParams(nl, (C.c_int * (PTC_MAX_LAYERS + 1))(*channels), seed, init_scale, int(tensor_cores))
         self.ptr = _vp()
         check(lib().qkx_ptc_create(lat.ctx, C.byref(p), C.byref(self.ptr)))
         self.nw = int(lib().qkx_ptc_num_weights(self.ptr))

@@ -12,6 +12,7 @@
 #include "hop_mrhs.cuh"
 #include "layout.cuh"
 #include "ptc.cuh"
+#include "ptc_tc.cuh"
 #include "qkx_ctx.cuh"
 
 using namespace qkx;
@@ -35,6 +36,8 @@ struct qkx_ptc {
   double* red = nullptr;                     // reduction partials
   int red_n = 0;
   int adam_t = 0;
+  int use_tc = 0;          // 16 -> 16 inference layers on the tensor cores
+  int* tc_err = nullptr;   // device flag set by a timed-out tensor-core wait
 };
 
 namespace qkx {
@@ -76,6 +79,20 @@ int layer(qkx_ctx* c, int ci, int co, const float4* in, float4* out, const __nv_
   if (ci == A && co == B) layer_t<A, B>(c, in, out, w); else
   QKX_PTC_WIDTHS(QKX_L) return bad("channel widths");
 #undef QKX_L
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  return QKX_OK;
+}
+
+// 16 -> 16 layer on the tensor cores (ptc_tc.cuh)
+int layer_tc(qkx_ctx* c, const float4* in, float4* out, const __nv_bfloat162* w, int* err) {
+  static bool attr = false;
+  if (!attr) {
+    QKX_CUDA(cudaFuncSetAttribute(k_ptc_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
+    attr = true;
+  }
+  const int nb = 2 * ((c->Vh + TC_M - 1) / TC_M);
+  k_ptc_layer_tc<<<nb, TC_M, sizeof(TcSmem), c->st>>>(in, out, w, GaugeF32x12{c->U12f, c->Vh}, c->geom_raw, err);
   counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
@@ -310,13 +327,31 @@ int refresh_backward_weights(qkx_ptc* n) {
   return QKX_OK;
 }
 
-// out = N(in); the layer outputs are kept in act[1..nl-1] for the backward pass
-int forward(qkx_ptc* n, const float4* in, float4* out) {
+// out = N(in); the layer outputs are kept in act[1..nl-1] for the backward pass.
+// With tc (inference only) the 16 -> 16 layers run on the tensor cores.
+int forward(qkx_ptc* n, const float4* in, float4* out, bool tc = false) {
   const float4* src = in;
   for (int l = 0; l < n->nl; l++) {
     float4* dst = (l == n->nl - 1) ? out : n->act[l + 1];
-    QKX_TRY(layer(n->c, n->ch[l], n->ch[l + 1], src, dst, n->wb + n->woff[l]));
+    if (tc && n->ch[l] == 16 && n->ch[l + 1] == 16)
+      QKX_TRY(layer_tc(n->c, src, dst, n->wb + n->woff[l], n->tc_err));
+    else
+      QKX_TRY(layer(n->c, n->ch[l], n->ch[l + 1], src, dst, n->wb + n->woff[l]));
     src = dst;
+  }
+  return QKX_OK;
+}
+
+// the tensor-core error flag, cleared after reading
+int check_tc(qkx_ptc* n) {
+  if (!n->use_tc) return QKX_OK;
+  int h = 0;
+  QKX_CUDA(cudaMemcpyAsync(&h, n->tc_err, sizeof(int), cudaMemcpyDeviceToHost, n->c->st));
+  QKX_CUDA(cudaStreamSynchronize(n->c->st));
+  if (h) {
+    QKX_CUDA(cudaMemsetAsync(n->tc_err, 0, sizeof(int), n->c->st));
+    set_error("tensor-core PTC layer: an mbarrier wait timed out");
+    return QKX_ERR_CUDA;
   }
   return QKX_OK;
 }
@@ -558,7 +593,7 @@ int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
       double rho2 = r2;
       for (int k = 0; k < GCR_M && rc == QKX_OK; k++) {
         if (net) {
-          if (forward(net, rho, Zv[k]) != QKX_OK) {
+          if (forward(net, rho, Zv[k], net->use_tc != 0) != QKX_OK) {
             fail(QKX_ERR_CUDA);
             break;
           }
@@ -639,6 +674,7 @@ int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
   cudaEventElapsedTime(&ms, e0, e1);
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  if (rc == QKX_OK && net) rc = check_tc(net);
   if (rc != QKX_OK) return rc;
   if (info) {
     info->iterations = total_it;
@@ -668,6 +704,7 @@ int qkx_ptc_create(qkx_ctx* c, const qkx_ptc_params* p, qkx_ptc** out) {
   QKX_CUDA(cudaSetDevice(c->device));
   qkx_ptc* n = new qkx_ptc;
   n->c = c;
+  n->use_tc = p->tensor_cores ? 1 : 0;
   n->nl = p->nlayers;
   for (int l = 0; l <= n->nl; l++) n->ch[l] = p->channels[l];
   for (int l = 0; l < n->nl; l++) {
@@ -677,8 +714,10 @@ int qkx_ptc_create(qkx_ctx* c, const qkx_ptc_params* p, qkx_ptc** out) {
   int rc = QKX_OK;
   if (dalloc(&n->w, n->nw, "PTC weights") || dalloc(&n->m, n->nw, "Adam moments") ||
       dalloc(&n->v, n->nw, "Adam moments") || dalloc(&n->wb, n->nw, "BF16 weights") ||
-      dalloc(&n->wt, n->nw, "BF16 weights") || dalloc(&n->grad, n->nw, "weight gradient"))
+      dalloc(&n->wt, n->nw, "BF16 weights") || dalloc(&n->grad, n->nw, "weight gradient") ||
+      dalloc(&n->tc_err, 1, "error flag"))
     rc = QKX_ERR_NOMEM;
+  if (rc == QKX_OK && cudaMemsetAsync(n->tc_err, 0, sizeof(int), c->st) != cudaSuccess) rc = QKX_ERR_CUDA;
   if (rc != QKX_OK) {
     qkx_ptc_destroy(n);
     return rc;
@@ -721,6 +760,7 @@ void qkx_ptc_destroy(qkx_ptc* n) {
   cudaFree(n->wb);
   cudaFree(n->wt);
   cudaFree(n->grad);
+  cudaFree(n->tc_err);
   cudaFree(n->part);
   cudaFree(n->red);
   for (int l = 0; l <= QKX_PTC_MAX_LAYERS; l++) cudaFree(n->act[l]);
@@ -785,7 +825,8 @@ int qkx_ptc_apply(qkx_ptc* n, const double* in_host, double* out_host) {
     return QKX_ERR_NOMEM;
   }
   int rc = upload_f32(n, in_host, a, c->w[0]);
-  if (rc == QKX_OK) rc = forward(n, a, y);
+  if (rc == QKX_OK) rc = forward(n, a, y, n->use_tc != 0);
+  if (rc == QKX_OK) rc = check_tc(n);
   if (rc == QKX_OK) {
     k_f32_to_f64<<<fgrid((size_t)12 * c->Vh), FNT, 0, c->st>>>(y, c->w[1], c->Vh);
     counted(c);

@@ -4,9 +4,11 @@ training on the library's own solves, and the flexible GCR solver that uses it
 (true residual checked in FP64 by the oracle, gain over no preconditioner, and
 the plain-solver fallback).
 
-Tolerances: the kernels compute in FP32 (BF16 weights, FP32 activations,
-FP32 tile sums, FP64 across tiles), the oracle in FP64 at the same weights:
-forward 1e-5 relative, loss 1e-5, gradient 1e-4 (norm-relative)."""
+Tolerances: the training kernels compute in FP32 (BF16 weights, FP32
+activations, FP32 tile sums, FP64 across tiles), the oracle in FP64 at the
+same weights: forward 1e-5 relative, loss 1e-5, gradient 1e-4 (norm-relative).
+The tensor-core inference layer also rounds the transported activations to
+BF16 (relative rounding 2^-9): 1e-2 against both."""
 import numpy as np
 import pytest
 
@@ -31,7 +33,7 @@ def setup(qkx, oracle):
 @pytest.mark.parametrize("ch", [CH, (4, 8, 4), (4, 16, 8, 4)])
 def test_forward_matches_oracle(qkx, oracle, setup, ch):
     lat, U = setup
-    net = qkx.Ptc(lat, ch, seed=11, init_scale=0.3)
+    net = qkx.Ptc(lat, ch, seed=11, init_scale=0.3, tensor_cores=False)
     W = net.weights(1)
     for seed in (1, 2):
         r = oracle.spinor_gaussian(L, seed)
@@ -41,9 +43,28 @@ def test_forward_matches_oracle(qkx, oracle, setup, ch):
     net.close()
 
 
+@pytest.mark.parametrize("Lt", [(4, 4, 4, 8), (6, 4, 2, 10), (8, 8, 8, 16)])
+def test_tensor_core_layer(qkx, oracle, Lt):
+    """tcgen05 16 -> 16 layers (BF16 activations) against the FP32 kernels and the oracle,
+    including a lattice whose half volume is not a multiple of the 128-site tile."""
+    U = oracle.apply_bc(Lt, oracle.gauge_random(Lt, 0.3, 31), -1)
+    with qkx.Lattice(qkx.LatticeInfo(L=Lt, kappa=KAPPA, mu=MU)) as lat:
+        lat.load_gauge(U, qkx.LINKS_AS_GIVEN)
+        ref = qkx.Ptc(lat, CH, seed=12, init_scale=0.3, tensor_cores=False)
+        tc = qkx.Ptc(lat, CH, seed=99, init_scale=0.3, tensor_cores=True)
+        tc.set_weights(ref.weights(0))
+        r = oracle.spinor_gaussian(Lt, 6)
+        a, b = ref.apply(r), tc.apply(r)
+        assert rel(b, a) < 1e-2, rel(b, a)
+        assert rel(b, oracle.ptc_forward(Lt, U, list(CH), ref.weights(1), r)) < 1e-2
+        assert rel(a, oracle.ptc_forward(Lt, U, list(CH), ref.weights(1), r)) < 1e-5
+        ref.close()
+        tc.close()
+
+
 def test_identity_at_zero_init(qkx, oracle, setup):
     lat, _ = setup
-    net = qkx.Ptc(lat, CH, seed=1, init_scale=0.0)
+    net = qkx.Ptc(lat, CH, seed=1, init_scale=0.0, tensor_cores=False)
     r = oracle.spinor_gaussian(L, 3)
     assert rel(net.apply(r), r) < 1e-7
     net.close()
