@@ -294,6 +294,65 @@ QKX_API int qkx_gaussian_smear(qkx_ctx* ctx, int nrhs, const double* const* in_h
 QKX_API int qkx_gaussian_smear_dev(qkx_ctx* ctx, int nrhs, const double* const* in_dev, double* const* out_dev,
                                    int nsmear, double alpha);
 
+/* ---------------------------------------------------------------- two-point functions
+ * From propagators in the Propagator::M layout (host, or device memory for the
+ * _dev forms, e.g. the output of qkx_propagator_dev).  Momenta p = 2 pi n / L
+ * are those of createMomenta (lib/contractions.cpp:37): every integer n with
+ * |n|^2 = q for q = 0..Q_sq, each component running from +q down to -q; the
+ * Fourier transform is sum_x C(x) exp(-i p.(x - x_src)) over each time slice,
+ * with the reference's pi = 3.14159265359 and x - x_src not wrapped. */
+#define QKX_NUM_MESONS 10   /* MESONS_OPERATOR order: ONE G5 G1 G2 G3 G4 G5G1 G5G2 G5G3 G5G4 */
+#define QKX_BARYON_NTN 0    /* BARYON_OPERATOR order */
+#define QKX_BARYON_NTR 1
+#define QKX_BARYON_RTN 2
+#define QKX_BARYON_RTR 3
+
+/* createMomenta: writes up to max momenta as mom[i][3] and returns their number */
+QKX_API int qkx_momenta(int Q_sq, int* mom, int max);
+/* Meson::contract(prop, op) + Meson::fourier(FORWARD) (lib/contractions.cpp:251,
+ * :121) for nop operators: corr[op][t][imom] complex (Meson::F per operator). */
+QKX_API int qkx_meson_2pt(qkx_ctx* ctx, const double* prop_host, int nop, const int* ops, int Q_sq,
+                          const int x_src[4], double* corr);
+QKX_API int qkx_meson_2pt_dev(qkx_ctx* ctx, const double* prop_dev, int nop, const int* ops, int Q_sq,
+                              const int x_src[4], double* corr);
+/* Baryon::contract(prop1, prop2, op) + Baryon::fourier(FORWARD) (lib/contractions.cpp:494,
+ * :356): corr[t][imom][gamma][gamma'] complex (Baryon::F). */
+QKX_API int qkx_baryon_2pt(qkx_ctx* ctx, const double* prop1_host, const double* prop2_host, int op, int Q_sq,
+                           const int x_src[4], double* corr);
+QKX_API int qkx_baryon_2pt_dev(qkx_ctx* ctx, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
+                               const int x_src[4], double* corr);
+
+/* ---------------------------------------------------------------- ILDG / LIME configurations
+ * A LIME file is a sequence of records, each a 144-byte big-endian header
+ * (magic 0x456789ab, version, MB/ME flags, data length, 128-byte type string)
+ * followed by its data padded to a multiple of 8 bytes.  An ILDG gauge
+ * configuration has an "ildg-format" XML record (<precision>, <lx> .. <lt>)
+ * and an "ildg-binary-data" record: V x 4 x 3 x 3 big-endian complex numbers,
+ * sites with x fastest and t slowest, directions x y z t -- the Gauge::M
+ * layout once byte-swapped. */
+typedef struct qkx_lime_info {
+  int precision;            /* 64 or 32 (bits per real), from the ildg-format record (64 if absent) */
+  int L[4];                 /* lattice extents from the ildg-format record (0 if absent) */
+  long long data_offset;    /* byte offset of the binary data in the file */
+  long long data_bytes;     /* its length */
+  int records;              /* records scanned */
+} qkx_lime_info;
+
+/* qkxTM_MPI_getGaugeLime(fname, u) (lib/read_conf_lime.cpp:111-245): read the
+ * ildg-binary-data record of an ILDG file into the context as its operator
+ * links (bc_mode as in qkx_load_gauge) and, if U_host is not NULL, into U_host
+ * (Gauge::M layout).  The file is streamed through two page-locked buffers, so
+ * disk reads overlap the host-to-device copies; the byte swap and the layout
+ * change run on the GPU.  Beyond the reference: 32-bit files are accepted
+ * (converted to FP64), and the extents in the ildg-format record must match
+ * the context's lattice. */
+QKX_API int qkx_read_gauge_lime(qkx_ctx* ctx, const char* path, int bc_mode, double* U_host, qkx_lime_info* info);
+/* qkxTM_writeGaugeLime(fname, u, message) (lib/write_conf_lime.cpp:49-199):
+ * write an ILDG file with the records ildg-format (64-bit), xlf-info (message)
+ * and ildg-binary-data.  U_host (Gauge::M layout) is written, or the context's
+ * operator links as stored when U_host is NULL. */
+QKX_API int qkx_write_gauge_lime(qkx_ctx* ctx, const char* path, const double* U_host, const char* message);
+
 /* ---------------------------------------------------------------- propagators
  * A propagator is double[V][4 mu][4 nu][3 c1][3 c2][2] (Propagator::M,
  * include/lattice_util.h:168), site order LEXIC; V*2304 bytes. */

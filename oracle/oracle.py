@@ -95,6 +95,9 @@ def lib():
         L.orc_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
         L.orc_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
         L.orc_absorb_vector.argtypes = [C.c_long, _dp, C.c_int, C.c_int, _dp]
+        L.orc_momenta.argtypes = [C.c_int, _ip, C.c_int]
+        L.orc_meson_2pt.argtypes = [_ip, _dp, C.c_int, C.c_int, _ip, _dp]
+        L.orc_baryon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
         L.orc_ptc_nweights.argtypes = [C.c_int, _ip]
         L.orc_ptc_nweights.restype = C.c_long
         L.orc_ptc_forward.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
@@ -124,6 +127,8 @@ def ref():
         _ref.ref_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
         _ref.ref_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
         _ref.ref_absorb_vector.argtypes = [_ip, _dp, C.c_int, C.c_int, _dp]
+        _ref.ref_meson_2pt.argtypes = [_ip, _dp, C.c_int, C.c_int, _ip, _dp]
+        _ref.ref_baryon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
         _ref.ref_propagator.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                         _dp, _dp, C.c_int, C.c_double, C.c_long, _dp]
     return _ref
@@ -356,3 +361,47 @@ def ptc_loss_grad(L, U, ch, W, r, e, grad=True):
                                    _ptr(np.ascontiguousarray(r)), _ptr(np.ascontiguousarray(e)),
                                    _ptr(g) if grad else None)
     return loss, g
+
+
+# ---------------------------------------------------------------- contractions
+MESONS = ["ONE", "G5", "G1", "G2", "G3", "G4", "G5G1", "G5G2", "G5G3", "G5G4"]
+BARYONS = ["NTN", "NTR", "RTN", "RTR"]
+
+
+def momenta(Q_sq) -> np.ndarray:
+    """createMomenta (lib/contractions.cpp:37) as [Nmom, 3]."""
+    buf = np.zeros(3000, dtype=np.int32)
+    n = lib().orc_momenta(Q_sq, buf.ctypes.data_as(_ip), 1000)
+    return buf[:3 * n].reshape(n, 3).copy()
+
+
+def meson_2pt(L, prop, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    """Meson::contract + fourier(FORWARD): [Lt, Nmom, 2]."""
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 2))
+    lib().orc_meson_2pt(_L(L), _ptr(np.ascontiguousarray(prop)), op, Q_sq, _L(x_src), _ptr(out))
+    return out
+
+
+def baryon_2pt(L, prop1, prop2, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    """Baryon::contract + fourier(FORWARD): [Lt, Nmom, 4, 4, 2]."""
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 4, 4, 2))
+    lib().orc_baryon_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), op, Q_sq,
+                         _L(x_src), _ptr(out))
+    return out
+
+
+def ref_meson_2pt(L, prop, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 2))
+    ref().ref_meson_2pt(_L(L), _ptr(np.ascontiguousarray(prop)), op, Q_sq, _L(x_src), _ptr(out))
+    return out
+
+
+def ref_baryon_2pt(L, prop1, prop2, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 4, 4, 2))
+    ref().ref_baryon_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), op, Q_sq,
+                         _L(x_src), _ptr(out))
+    return out

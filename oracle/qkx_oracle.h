@@ -87,6 +87,15 @@ void orc_gaussian_smear(const int L[4], const double* U, const double* in, doubl
                         double alpha);
 void orc_absorb_vector(long V, const double* phi, int nu, int c2, double* prop);
 
+/* two-point contractions (qkx_oracle_contract.c): createMomenta
+ * (lib/contractions.cpp:37), Meson::contract + fourier(FORWARD) (:251, :121),
+ * Baryon::contract + fourier(FORWARD) (:494, :356).  Return the number of
+ * momenta; corr is [Lt][Nmom] (meson) or [Lt][Nmom][4][4] (baryon) complex. */
+int orc_momenta(int Q_sq, int* mom, int max);
+int orc_meson_2pt(const int L[4], const double* prop, int op, int Q_sq, const int x_src[4], double* corr);
+int orc_baryon_2pt(const int L[4], const double* prop1, const double* prop2, int op, int Q_sq, const int x_src[4],
+                   double* corr);
+
 /* learned preconditioner (qkx_oracle_ptc.c; no reference counterpart): a linear
  * parallel-transport convolution network with nlayers layers of channel widths
  * ch[0..nlayers]; weights [9][ch[l+1]][ch[l]] complex per layer, concatenated. */

@@ -326,4 +326,48 @@ void ref_propagator(const int L[4], double kappa, double mu, int twistSign, doub
   memcpy(prop, &(p.M[0][0][0][0][0]), sizeof(double) * 288 * volume(L));
 }
 
+/* Meson::contract(prop, op) and fourier(FORWARD) (lib/contractions.cpp:251, :121)
+ * with Q_sq and x_src; corr receives Meson::F ([Lt][Nmom] complex).  Returns Nmom. */
+int ref_meson_2pt(const int L[4], const double* prop, int op, int Q_sq, const int x_src[4], double* corr) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  li.Q_sq = Q_sq;
+  for (int i = 0; i < 4; i++) li.x_src[i] = x_src[i];
+  Propagator p(&li);
+  memcpy(&(p.M[0][0][0][0][0]), prop, sizeof(double) * 288 * volume(L));
+  char devnull[] = "/dev/null";
+  int nmom;
+  {
+    QuietStdout q;
+    Meson m(&li, devnull);
+    m.contract(p, (MESONS_OPERATOR)op);
+    m.fourier(FORWARD);
+    nmom = m.Nmom;
+    memcpy(corr, m.F, sizeof(double) * 2 * L[3] * nmom);
+  }
+  return nmom;
+}
+
+/* Baryon::contract(prop1, prop2, op) and fourier(FORWARD) (lib/contractions.cpp:494,
+ * :356); corr receives Baryon::F ([Lt][Nmom][4][4] complex).  Returns Nmom. */
+int ref_baryon_2pt(const int L[4], const double* prop1, const double* prop2, int op, int Q_sq, const int x_src[4],
+                   double* corr) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  li.Q_sq = Q_sq;
+  for (int i = 0; i < 4; i++) li.x_src[i] = x_src[i];
+  Propagator p1(&li), p2(&li);
+  memcpy(&(p1.M[0][0][0][0][0]), prop1, sizeof(double) * 288 * volume(L));
+  memcpy(&(p2.M[0][0][0][0][0]), prop2, sizeof(double) * 288 * volume(L));
+  char devnull[] = "/dev/null";
+  int nmom;
+  {
+    QuietStdout q;
+    Baryon b(&li, devnull);
+    b.contract(p1, p2, (BARYON_OPERATOR)op);
+    b.fourier(FORWARD);
+    nmom = b.Nmom;
+    memcpy(corr, b.F, sizeof(double) * 32 * L[3] * nmom);
+  }
+  return nmom;
+}
+
 }  // extern "C"

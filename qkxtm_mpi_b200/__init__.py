@@ -72,6 +72,8 @@ SYMBOLS = [
     "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
     "qkx_ptc_set_weights", "qkx_ptc_apply", "qkx_ptc_loss_grad", "qkx_ptc_train",
+    "qkx_read_gauge_lime", "qkx_write_gauge_lime", "qkx_momenta", "qkx_meson_2pt", "qkx_meson_2pt_dev",
+    "qkx_baryon_2pt", "qkx_baryon_2pt_dev",
 ]
 
 
@@ -112,6 +114,11 @@ class PtcTrainInfo(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class LimeInfo(C.Structure):
+    _fields_ = [("precision", C.c_int), ("L", C.c_int * 4), ("data_offset", C.c_longlong),
+                ("data_bytes", C.c_longlong), ("records", C.c_int)]
 
 
 class SolveInfo(C.Structure):
@@ -205,6 +212,13 @@ def lib() -> C.CDLL:
         L.qkx_ptc_apply.argtypes = [_vp, _vp, _vp]
         L.qkx_ptc_loss_grad.argtypes = [_vp, _vp, _vp, _dp, _vp]
         L.qkx_ptc_train.argtypes = [_vp, C.POINTER(PtcTrainParams), C.POINTER(PtcTrainInfo)]
+        L.qkx_read_gauge_lime.argtypes = [_vp, C.c_char_p, C.c_int, _vp, C.POINTER(LimeInfo)]
+        L.qkx_write_gauge_lime.argtypes = [_vp, C.c_char_p, _vp, C.c_char_p]
+        L.qkx_momenta.argtypes = [C.c_int, _vp, C.c_int]
+        L.qkx_meson_2pt.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_int), _vp]
+        L.qkx_meson_2pt_dev.argtypes = L.qkx_meson_2pt.argtypes
+        L.qkx_baryon_2pt.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(C.c_int), _vp]
+        L.qkx_baryon_2pt_dev.argtypes = L.qkx_baryon_2pt.argtypes
         _lib = L
     return _lib
 
@@ -318,6 +332,21 @@ class Lattice:
 
     def generate_gauge(self, eps: float, seed: int, bc_mode: int = LINKS_APPLY_BC) -> None:
         check(lib().qkx_gauge_generate(self.ctx, eps, seed, bc_mode))
+
+    def read_gauge_lime(self, path: str, bc_mode: int = LINKS_AS_GIVEN, want_host: bool = True):
+        """qkxTM_MPI_getGaugeLime: load an ILDG file as the operator's links.
+        Returns (Gauge::M array or None, info dict)."""
+        U = np.empty((self.V, 4, 3, 3, 2)) if want_host else None
+        info = LimeInfo()
+        check(lib().qkx_read_gauge_lime(self.ctx, os.fsencode(path), bc_mode,
+                                        U.ctypes.data if want_host else None, C.byref(info)))
+        return U, {"precision": info.precision, "L": tuple(info.L), "data_offset": info.data_offset,
+                   "data_bytes": info.data_bytes, "records": info.records}
+
+    def write_gauge_lime(self, path: str, U: np.ndarray | None = None, message: str = "") -> None:
+        """qkxTM_writeGaugeLime: write U (or the operator's links as stored) as an ILDG file."""
+        check(lib().qkx_write_gauge_lime(self.ctx, os.fsencode(path), _host(U).ctypes.data if U is not None else None,
+                                         message.encode()))
 
     def download_gauge(self) -> np.ndarray:
         U = np.empty((self.V, 4, 3, 3, 2))
@@ -509,6 +538,28 @@ class Lattice:
                                        prop_ptr, C.byref(info)))
         return info
 
+    # ------------------------------------------------------------ two-point functions
+    def meson_2pt(self, prop, ops=tuple(range(10)), Q_sq: int = 0, x_src=(0, 0, 0, 0), device: bool = False):
+        """Meson::contract + fourier(FORWARD) for the operators ops: [nop, Lt, Nmom, 2].
+        prop is a host array, or with device=True a device pointer (int)."""
+        ops = list(ops)
+        nmom = len(momenta(Q_sq))
+        out = np.zeros((len(ops), self.info.L[3], nmom, 2))
+        f = lib().qkx_meson_2pt_dev if device else lib().qkx_meson_2pt
+        ptr = prop if device else _host(prop).ctypes.data
+        check(f(self.ctx, ptr, len(ops), (C.c_int * len(ops))(*ops), Q_sq, (C.c_int * 4)(*x_src), out.ctypes.data))
+        return out
+
+    def baryon_2pt(self, prop1, prop2, op: int, Q_sq: int = 0, x_src=(0, 0, 0, 0), device: bool = False):
+        """Baryon::contract(prop1, prop2, op) + fourier(FORWARD): [Lt, Nmom, 4, 4, 2]."""
+        nmom = len(momenta(Q_sq))
+        out = np.zeros((self.info.L[3], nmom, 4, 4, 2))
+        f = lib().qkx_baryon_2pt_dev if device else lib().qkx_baryon_2pt
+        p1 = prop1 if device else _host(prop1).ctypes.data
+        p2 = prop2 if device else _host(prop2).ctypes.data
+        check(f(self.ctx, p1, p2, op, Q_sq, (C.c_int * 4)(*x_src), out.ctypes.data))
+        return out
+
     # ------------------------------------------------------------ profiling
     def profile(self, on: bool) -> None:
         check(lib().qkx_profile_enable(self.ctx, int(on)))
@@ -593,6 +644,20 @@ class Ptc:
         info = PtcTrainInfo()
         check(lib().qkx_ptc_train(self.ptr, C.byref(tp), C.byref(info)))
         return info.as_dict()
+
+
+MESONS = ["ONE", "G5", "G1", "G2", "G3", "G4", "G5G1", "G5G2", "G5G3", "G5G4"]
+BARYONS = ["NTN", "NTR", "RTN", "RTR"]
+
+
+def momenta(Q_sq: int) -> np.ndarray:
+    """createMomenta (lib/contractions.cpp:37) as [Nmom, 3]."""
+    n = lib().qkx_momenta(Q_sq, None, 0)
+    if n < 0:
+        check(n)
+    m = np.zeros((n, 3), dtype=np.int32)
+    lib().qkx_momenta(Q_sq, m.ctypes.data, n)
+    return m
 
 
 def pinned_array(shape) -> np.ndarray:

@@ -380,7 +380,7 @@ int download_spinor(qkx_ctx* c, const double2* dev, double* host) {
 // Check the links the operator uses and, if they are SU(3) up to one global
 // sign on the last time slice's t-links, build the 12-real FP32/FP16 copies
 // with that sign stripped (the kernels then apply it from the coordinate).
-static int gauge_finish(qkx_ctx* c) {
+int gauge_finish(qkx_ctx* c) {
   const int nl = 8 * c->Vh;
   const int nb = (nl + 255) / 256;
   double* part = nullptr;

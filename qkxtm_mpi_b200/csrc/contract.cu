@@ -1,0 +1,437 @@
+// contract.cu -- meson and nucleon two-point functions from propagators
+// (lib/contractions.cpp: Meson::contract :251, Baryon::contract :494, their
+// fourier(FORWARD) :121 / :356 and createMomenta :37) on one B200.
+//
+// A propagator is [V][4][4][3][3] complex in the host layout (Propagator::M).
+// Per site the contraction needs the whole site block (2304 bytes per
+// propagator), so blocks stage 16 sites' blocks in shared memory with
+// coalesced loads and then compute:
+//   mesons   one thread per (site, operator)
+//   nucleons one thread per (site, gamma, gamma'), each walking the tabulated
+//            spin terms of its (gamma, gamma') and the 36 colour permutations.
+// The terms are tabulated on the host in the reference's order (same
+// threshold |value|^2 > 1e-3) from the gamma and charge-conjugation matrices
+// of lib/lattice_util.cpp:255-305.  The Fourier transform is one block per
+// (time slice, momentum) with the reference's phase convention:
+//   F[t][p] = sum_x C(x) exp(-2 pi i sum_mu p_mu (x_mu - x_src_mu) / L_mu),
+// pi = 3.14159265359 as in lib/contractions.cpp:5, x - x_src not wrapped.
+#include <string.h>
+
+#include <algorithm>
+#include <complex>
+#include <vector>
+
+#include "qkx_ctx.cuh"
+
+using namespace qkx;
+
+namespace qkx {
+namespace {
+
+constexpr int CT_SITES = 16;           // sites per block
+constexpr double REF_PI = 3.14159265359;
+using zc = std::complex<double>;
+
+int bad(const char* what) {
+  set_error("invalid argument: %s", what);
+  return QKX_ERR_INVALID;
+}
+
+// ---------------------------------------------------------------- host tables
+struct Gammas {
+  zc G[5][4][4], C[4][4], Cbar[4][4], CG[5][4][4], CGbar[5][4][4];
+  Gammas() {  // std::complex members start at zero
+    const zc j(0, 1);
+    G[0][0][3] = j, G[0][1][2] = j, G[0][2][1] = -j, G[0][3][0] = -j;
+    G[1][0][3] = 1, G[1][1][2] = -1, G[1][2][1] = -1, G[1][3][0] = 1;
+    G[2][0][2] = j, G[2][1][3] = -j, G[2][2][0] = -j, G[2][3][1] = j;
+    G[3][0][0] = 1, G[3][1][1] = 1, G[3][2][2] = -1, G[3][3][3] = -1;
+    G[4][0][2] = 1, G[4][1][3] = 1, G[4][2][0] = 1, G[4][3][1] = 1;
+    for (int m = 0; m < 4; m++)
+      for (int n = 0; n < 4; n++)
+        for (int k = 0; k < 4; k++) C[m][n] += G[1][m][k] * G[3][k][n];
+    for (int m = 0; m < 4; m++)
+      for (int n = 0; n < 4; n++)
+        for (int k = 0; k < 4; k++)
+          for (int l = 0; l < 4; l++) Cbar[m][n] += G[3][m][l] * std::conj(C[k][l]) * G[3][k][n];
+    for (int i = 0; i < 5; i++)
+      for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++)
+          for (int k = 0; k < 4; k++) CG[i][m][n] += C[m][k] * G[i][k][n];
+    for (int i = 0; i < 5; i++)
+      for (int m = 0; m < 4; m++)
+        for (int n = 0; n < 4; n++)
+          for (int k = 0; k < 4; k++)
+            for (int l = 0; l < 4; l++) CGbar[i][m][n] += G[3][m][l] * std::conj(CG[i][k][l]) * G[3][k][n];
+  }
+};
+
+bool keep(zc v) { return std::norm(v) > 1e-3; }
+
+// ---- mesons: per operator, terms (value; beta, gamma, delta, alpha) in tabulateIndices order
+constexpr int MESON_MAX_TERMS = 64;
+struct MesonTerms {
+  int n;
+  double2 val[MESON_MAX_TERMS];
+  char4 ind[MESON_MAX_TERMS];  // beta, gamma, delta, alpha
+};
+
+void meson_terms(const Gammas& g, int op, MesonTerms& t) {
+  zc m[4][4] = {};
+  if (op == 0) {
+    for (int i = 0; i < 4; i++) m[i][i] = 1;
+  } else if (op == 1) {
+    memcpy((void*)m, g.G[4], sizeof m);
+  } else if (op <= 5) {
+    memcpy((void*)m, g.G[op - 2], sizeof m);
+  } else {
+    for (int a = 0; a < 4; a++)
+      for (int b = 0; b < 4; b++)
+        for (int k = 0; k < 4; k++) m[a][b] += g.G[4][a][k] * g.G[op - 6][k][b];
+  }
+  t.n = 0;
+  for (int be = 0; be < 4; be++)
+    for (int ga = 0; ga < 4; ga++)
+      for (int de = 0; de < 4; de++)
+        for (int al = 0; al < 4; al++) {
+          const zc v = m[be][ga] * m[de][al];
+          if (keep(v) && t.n < MESON_MAX_TERMS) {
+            t.val[t.n] = make_double2(v.real(), v.imag());
+            t.ind[t.n] = make_char4(be, ga, de, al);
+            t.n++;
+          }
+        }
+}
+
+// ---- nucleons: per (gamma, gamma'), terms (value; alpha, beta, beta', alpha', X, Y)
+// with X, Y the spins of the third quark's propagator element (see orc_baryon_2pt)
+constexpr int BARYON_MAX_TERMS = 64;
+struct BaryonTerms {
+  int n[16];
+  double2 val[16][BARYON_MAX_TERMS];
+  char4 ab[16][BARYON_MAX_TERMS];  // alpha, beta, beta', alpha'
+  char2 xy[16][BARYON_MAX_TERMS];  // X, Y
+};
+
+int baryon_terms(const Gammas& g, int op, BaryonTerms& t) {
+  memset(t.n, 0, sizeof t.n);
+  auto add = [&](int gg, int gp, zc v, int al, int be, int bp, int ap, int X, int Y) -> int {
+    const int k = gg * 4 + gp;
+    if (t.n[k] >= BARYON_MAX_TERMS) return QKX_ERR_INVALID;
+    t.val[k][t.n[k]] = make_double2(v.real(), v.imag());
+    t.ab[k][t.n[k]] = make_char4(al, be, bp, ap);
+    t.xy[k][t.n[k]] = make_char2(X, Y);
+    t.n[k]++;
+    return QKX_OK;
+  };
+  for (int gg = 0; gg < 4; gg++)
+    for (int gp = 0; gp < 4; gp++)
+      for (int al = 0; al < 4; al++)
+        for (int be = 0; be < 4; be++)
+          for (int bp = 0; bp < 4; bp++)
+            for (int ap = 0; ap < 4; ap++) {
+              if (op == 0) {
+                const zc v = g.CG[4][al][be] * g.CGbar[4][bp][ap];
+                if (keep(v)) QKX_TRY(add(gg, gp, v, al, be, bp, ap, gg, gp));
+              } else if (op == 1) {  // gamma' from the term, delta' the third quark's source spin
+                for (int dp = 0; dp < 4; dp++) {
+                  const zc v = g.CG[4][al][be] * g.Cbar[bp][ap] * g.G[4][gp][dp];
+                  if (keep(v)) QKX_TRY(add(gg, gp, v, al, be, bp, ap, gg, dp));
+                }
+              } else if (op == 2) {  // gamma from the term, delta the third quark's sink spin
+                for (int de = 0; de < 4; de++) {
+                  const zc v = g.C[al][be] * g.CGbar[4][bp][ap] * g.G[4][gg][de];
+                  if (keep(v)) QKX_TRY(add(gg, gp, v, al, be, bp, ap, de, gp));
+                }
+              } else {
+                for (int de = 0; de < 4; de++)
+                  for (int dp = 0; dp < 4; dp++) {
+                    const zc v = g.C[al][be] * g.Cbar[bp][ap] * g.G[4][gg][de] * g.G[4][gp][dp];
+                    if (keep(v)) QKX_TRY(add(gg, gp, v, al, be, bp, ap, de, dp));
+                  }
+              }
+            }
+  return QKX_OK;
+}
+
+// The reference accumulates each (gamma, gamma') over its terms in the
+// order of the tabulated index list; the loops above visit (alpha, beta,
+// beta', alpha') in that list's order and, within it, the free spins in the
+// list's order, so each per-(gamma, gamma') list keeps the reference's order.
+
+// ---------------------------------------------------------------- device
+__device__ __forceinline__ double2 cm(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+
+// stage CT_SITES site blocks (144 complex each) of a propagator into shared memory
+__device__ __forceinline__ void stage(double2* sp, const double2* __restrict__ prop, size_t s0, size_t V) {
+  const size_t base = s0 * 144;
+  const size_t total = (size_t)CT_SITES * 144;
+  for (size_t i = threadIdx.x; i < total; i += blockDim.x) {
+    const size_t site = s0 + i / 144;
+    sp[i] = site < V ? __ldg(prop + base + i) : make_double2(0.0, 0.0);
+  }
+}
+
+// C[op][site], block = CT_SITES sites x nop operators
+__global__ void k_meson_sites(const double2* __restrict__ prop, size_t V, int nop, const MesonTerms* __restrict__ T,
+                              double2* __restrict__ C) {
+  __shared__ double2 sp[CT_SITES * 144];
+  const size_t s0 = (size_t)blockIdx.x * CT_SITES;
+  stage(sp, prop, s0, V);
+  __syncthreads();
+  const int ls = threadIdx.x % CT_SITES, o = threadIdx.x / CT_SITES;
+  const size_t site = s0 + ls;
+  if (o >= nop || site >= V) return;
+  const double2* pp = sp + ls * 144;  // [mu][nu][c1][c2] at mu*36 + nu*9 + c1*3 + c2
+  const MesonTerms& t = T[o];
+  double2 m = make_double2(0.0, 0.0);
+  for (int a = 0; a < 3; a++)
+    for (int b = 0; b < 3; b++)
+      for (int i = 0; i < t.n; i++) {
+        const char4 ix = t.ind[i];  // beta, gamma, delta, alpha
+        // (g5 pp^+ g5)[gamma][delta][b][a] = conj(pp[g5(delta)][g5(gamma)][a][b]), g5 swapping spins 0<->2, 1<->3
+        const double2 q = pp[((ix.z + 2) & 3) * 36 + ((ix.y + 2) & 3) * 9 + a * 3 + b];
+        const double2 v = cm(cm(t.val[i], pp[ix.w * 36 + ix.x * 9 + a * 3 + b]), make_double2(q.x, -q.y));
+        m.x += v.x;
+        m.y += v.y;
+      }
+  C[(size_t)o * V + site] = m;
+}
+
+__constant__ int c_eps[6][3] = {{0, 1, 2}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
+__constant__ int c_sgn[6] = {+1, +1, +1, -1, -1, -1};
+
+// C[gamma*4 + gamma'][site], block = CT_SITES sites x 16 spin pairs
+__global__ void __launch_bounds__(CT_SITES * 16) k_baryon_sites(const double2* __restrict__ p1,
+                                                                const double2* __restrict__ p2, size_t V, double sign,
+                                                                const BaryonTerms* __restrict__ T,
+                                                                double2* __restrict__ C) {
+  extern __shared__ double2 sb[];
+  double2* s1 = sb;
+  double2* s2 = sb + CT_SITES * 144;
+  const size_t s0 = (size_t)blockIdx.x * CT_SITES;
+  stage(s1, p1, s0, V);
+  stage(s2, p2, s0, V);
+  __syncthreads();
+  const int ls = threadIdx.x % CT_SITES, k = threadIdx.x / CT_SITES;
+  const size_t site = s0 + ls;
+  if (site >= V) return;
+  const double2* q1 = s1 + ls * 144;
+  const double2* q2 = s2 + ls * 144;
+  double2 m = make_double2(0.0, 0.0);
+  const int n = T->n[k];
+  for (int i = 0; i < n; i++) {
+    const double2 val = T->val[k][i];
+    const char4 ab = T->ab[k][i];  // alpha, beta, beta', alpha'
+    const char2 xy = T->xy[k][i];
+    for (int e1 = 0; e1 < 6; e1++) {
+      const int a = c_eps[e1][0], b = c_eps[e1][1], c = c_eps[e1][2];
+      for (int e2 = 0; e2 < 6; e2++) {
+        const int a1 = c_eps[e2][0], b1 = c_eps[e2][1], c1 = c_eps[e2][2];
+        const double f = (double)(c_sgn[e1] * c_sgn[e2]);
+        const double2 fv = make_double2(f * val.x, f * val.y);
+        const double2 x1 = cm(q1[ab.x * 36 + ab.w * 9 + a * 3 + a1], q1[xy.x * 36 + xy.y * 9 + c * 3 + c1]);
+        const double2 x2 = cm(q1[ab.x * 36 + xy.y * 9 + a * 3 + c1], q1[xy.x * 36 + ab.w * 9 + c * 3 + a1]);
+        const double2 t = cm(cm(fv, q2[ab.y * 36 + ab.z * 9 + b * 3 + b1]), make_double2(x1.x - x2.x, x1.y - x2.y));
+        m.x += sign * t.x;
+        m.y += sign * t.y;
+      }
+    }
+  }
+  C[(size_t)k * V + site] = m;
+}
+
+// F[t][p][k] = sum over the slice's sites of C[k][site] exp(-i theta), one block per (t, p)
+__global__ void k_fourier(const double2* __restrict__ C, int K, size_t V, const int* __restrict__ mom, int nmom,
+                          Geom g, int4 src, double2* __restrict__ F) {
+  const int t = blockIdx.x / nmom, p = blockIdx.x % nmom;
+  const int V3 = g.L[0] * g.L[1] * g.L[2];
+  const int nx = mom[3 * p], ny = mom[3 * p + 1], nz = mom[3 * p + 2];
+  double re[16], im[16];
+#pragma unroll
+  for (int k = 0; k < 16; k++) re[k] = im[k] = 0.0;
+  for (int s = threadIdx.x; s < V3; s += blockDim.x) {
+    const int x = s % g.L[0], y = (s / g.L[0]) % g.L[1], z = s / (g.L[0] * g.L[1]);
+    const double th =
+        (((double)nx * (x - src.x)) / g.L[0] + ((double)ny * (y - src.y)) / g.L[1] + ((double)nz * (z - src.z)) / g.L[2]) *
+        2 * REF_PI;
+    double sn, cs;
+    sincos(th, &sn, &cs);
+    const size_t v = (size_t)t * V3 + s;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+      if (k >= K) break;
+      const double2 c = C[(size_t)k * V + v];
+      re[k] += c.x * cs + c.y * sn;  // c * (cos - i sin)
+      im[k] += c.y * cs - c.x * sn;
+    }
+  }
+  for (int k = 0; k < K; k++) {
+    const double r = block_sum<256>(re[k]);
+    const double i = block_sum<256>(im[k]);
+    if (threadIdx.x == 0) F[((size_t)t * nmom + p) * K + k] = make_double2(r, i);
+  }
+}
+
+int host_momenta(int Q_sq, std::vector<int>& m) {
+  m.clear();
+  for (int q = 0; q <= Q_sq; q++)
+    for (int nx = q; nx >= -q; nx--)
+      for (int ny = q; ny >= -q; ny--)
+        for (int nz = q; nz >= -q; nz--)
+          if (nx * nx + ny * ny + nz * nz == q) m.insert(m.end(), {nx, ny, nz});
+  return (int)(m.size() / 3);
+}
+
+// a device copy of a host propagator (or the pointer itself for device input)
+struct PropIn {
+  const double2* d = nullptr;
+  void* owned = nullptr;
+};
+
+int prop_in(qkx_ctx* c, const double* p, bool host, PropIn& out) {
+  if (!host) {
+    out.d = (const double2*)p;
+    return QKX_OK;
+  }
+  const size_t bytes = sizeof(double2) * 144 * c->V;
+  if (cudaMallocAsync(&out.owned, bytes, c->st) != cudaSuccess) {
+    cudaGetLastError();
+    set_error("propagator copy: device allocation failed");
+    return QKX_ERR_NOMEM;
+  }
+  QKX_CUDA(cudaMemcpyAsync(out.owned, p, bytes, cudaMemcpyHostToDevice, c->st));
+  out.d = (const double2*)out.owned;
+  return QKX_OK;
+}
+
+// run the Fourier transform of C [K][V] and return F [Lt][nmom][K] to the host
+int fourier_to_host(qkx_ctx* c, const double2* C, int K, int Q_sq, const int x_src[4], double* out, int* nmom_out) {
+  std::vector<int> m;
+  const int nmom = host_momenta(Q_sq, m);
+  if (nmom > 1000) return bad("Q_sq gives more than 1000 momenta (MOM_MAX)");
+  int* dm = nullptr;
+  double2* F = nullptr;
+  const size_t nf = (size_t)c->p.L[3] * nmom * K;
+  QKX_CUDA(cudaMallocAsync((void**)&dm, sizeof(int) * m.size(), c->st));
+  QKX_CUDA(cudaMallocAsync((void**)&F, sizeof(double2) * nf, c->st));
+  QKX_CUDA(cudaMemcpyAsync(dm, m.data(), sizeof(int) * m.size(), cudaMemcpyHostToDevice, c->st));
+  k_fourier<<<c->p.L[3] * nmom, 256, 0, c->st>>>(C, K, c->V, dm, nmom, c->geom,
+                                                 make_int4(x_src[0], x_src[1], x_src[2], x_src[3]), F);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  QKX_CUDA(cudaMemcpyAsync(out, F, sizeof(double2) * nf, cudaMemcpyDeviceToHost, c->st));
+  QKX_CUDA(cudaFreeAsync(dm, c->st));
+  QKX_CUDA(cudaFreeAsync(F, c->st));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+  if (nmom_out) *nmom_out = nmom;
+  return QKX_OK;
+}
+
+int meson_2pt(qkx_ctx* c, const double* prop, bool host, int nop, const int* ops, int Q_sq, const int x_src[4],
+              double* corr) {
+  if (!c || !prop || !ops || !x_src || !corr) return bad("NULL argument");
+  if (nop < 1 || nop > QKX_NUM_MESONS) return bad("nop must be in 1..10");
+  for (int i = 0; i < nop; i++)
+    if (ops[i] < 0 || ops[i] >= QKX_NUM_MESONS) return bad("meson operator id");
+  if (Q_sq < 0) return bad("Q_sq < 0");
+  QKX_CUDA(cudaSetDevice(c->device));
+  static const Gammas g;
+  std::vector<MesonTerms> T(nop);
+  for (int i = 0; i < nop; i++) meson_terms(g, ops[i], T[i]);
+  PropIn pin;
+  QKX_TRY(prop_in(c, prop, host, pin));
+  MesonTerms* dT = nullptr;
+  double2* C = nullptr;
+  QKX_CUDA(cudaMallocAsync((void**)&dT, sizeof(MesonTerms) * nop, c->st));
+  QKX_CUDA(cudaMallocAsync((void**)&C, sizeof(double2) * nop * c->V, c->st));
+  QKX_CUDA(cudaMemcpyAsync(dT, T.data(), sizeof(MesonTerms) * nop, cudaMemcpyHostToDevice, c->st));
+  const unsigned nb = (unsigned)((c->V + CT_SITES - 1) / CT_SITES);
+  k_meson_sites<<<nb, CT_SITES * QKX_NUM_MESONS, 0, c->st>>>(pin.d, c->V, nop, dT, C);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  // Fourier per operator: K = 1 each, laid out [op][Lt][Nmom]
+  std::vector<int> m;
+  const int nmom = host_momenta(Q_sq, m);
+  int rc = QKX_OK;
+  for (int i = 0; i < nop && rc == QKX_OK; i++)
+    rc = fourier_to_host(c, C + (size_t)i * c->V, 1, Q_sq, x_src, corr + (size_t)i * 2 * c->p.L[3] * nmom, nullptr);
+  cudaFreeAsync(dT, c->st);
+  cudaFreeAsync(C, c->st);
+  if (pin.owned) cudaFreeAsync(pin.owned, c->st);
+  cudaStreamSynchronize(c->st);
+  return rc;
+}
+
+int baryon_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op, int Q_sq, const int x_src[4],
+               double* corr) {
+  if (!c || !p1 || !p2 || !x_src || !corr) return bad("NULL argument");
+  if (op < 0 || op > 3) return bad("baryon operator id");
+  if (Q_sq < 0) return bad("Q_sq < 0");
+  QKX_CUDA(cudaSetDevice(c->device));
+  static const Gammas g;
+  BaryonTerms T;
+  if (baryon_terms(g, op, T) != QKX_OK) return bad("internal: too many spin terms");
+  PropIn a, b;
+  QKX_TRY(prop_in(c, p1, host, a));
+  QKX_TRY(prop_in(c, p2, host, b));
+  BaryonTerms* dT = nullptr;
+  double2* C = nullptr;
+  QKX_CUDA(cudaMallocAsync((void**)&dT, sizeof(BaryonTerms), c->st));
+  QKX_CUDA(cudaMallocAsync((void**)&C, sizeof(double2) * 16 * c->V, c->st));
+  QKX_CUDA(cudaMemcpyAsync(dT, &T, sizeof(BaryonTerms), cudaMemcpyHostToDevice, c->st));
+  static bool attr = false;
+  const int smem = (int)(sizeof(double2) * 2 * CT_SITES * 144);
+  if (!attr) {
+    QKX_CUDA(cudaFuncSetAttribute(k_baryon_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const unsigned nb = (unsigned)((c->V + CT_SITES - 1) / CT_SITES);
+  const double sign = (op == 1 || op == 3) ? -1.0 : 1.0;
+  k_baryon_sites<<<nb, CT_SITES * 16, smem, c->st>>>(a.d, b.d, c->V, sign, dT, C);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  // F is [Lt][Nmom][16] = Baryon::F [Lt][Nmom][4][4]
+  const int rc = fourier_to_host(c, C, 16, Q_sq, x_src, corr, nullptr);
+  cudaFreeAsync(dT, c->st);
+  cudaFreeAsync(C, c->st);
+  if (a.owned) cudaFreeAsync(a.owned, c->st);
+  if (b.owned) cudaFreeAsync(b.owned, c->st);
+  cudaStreamSynchronize(c->st);
+  return rc;
+}
+
+}  // namespace
+}  // namespace qkx
+
+extern "C" {
+
+int qkx_momenta(int Q_sq, int* mom, int max) {
+  if (Q_sq < 0) return bad("Q_sq < 0");
+  std::vector<int> m;
+  const int n = host_momenta(Q_sq, m);
+  if (mom)
+    for (int i = 0; i < std::min(n, max) * 3; i++) mom[i] = m[i];
+  return n;
+}
+
+int qkx_meson_2pt(qkx_ctx* c, const double* prop_host, int nop, const int* ops, int Q_sq, const int x_src[4],
+                  double* corr) {
+  return meson_2pt(c, prop_host, true, nop, ops, Q_sq, x_src, corr);
+}
+int qkx_meson_2pt_dev(qkx_ctx* c, const double* prop_dev, int nop, const int* ops, int Q_sq, const int x_src[4],
+                      double* corr) {
+  return meson_2pt(c, prop_dev, false, nop, ops, Q_sq, x_src, corr);
+}
+int qkx_baryon_2pt(qkx_ctx* c, const double* prop1_host, const double* prop2_host, int op, int Q_sq,
+                   const int x_src[4], double* corr) {
+  return baryon_2pt(c, prop1_host, prop2_host, true, op, Q_sq, x_src, corr);
+}
+int qkx_baryon_2pt_dev(qkx_ctx* c, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
+                       const int x_src[4], double* corr) {
+  return baryon_2pt(c, prop1_dev, prop2_dev, false, op, Q_sq, x_src, corr);
+}
+
+}  // extern "C"

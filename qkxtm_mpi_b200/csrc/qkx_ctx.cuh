@@ -138,6 +138,8 @@ int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
 int ensure_stage(qkx_ctx* c);
 int ensure_links(qkx_ctx* c);
 int ensure_work(qkx_ctx* c);
+// after U18 changed: link checks, 12-real compression, solver caches invalidated
+int gauge_finish(qkx_ctx* c);
 // host Vector::M layout <-> device even-odd FP64 field, through the staging buffer
 int upload_spinor(qkx_ctx* c, const double* host, double2* dev);
 int download_spinor(qkx_ctx* c, const double2* dev, double* host);

@@ -20,7 +20,11 @@ Fixtures:
                       Vector::Gaussian_smearing and the propagator loop of
                       bin/test_invert_prop.cpp, lattice 4x4x4x8
 
-    python tests/golden/make_golden.py smear    (only ref_smear.npz)
+  ref_contract.npz    Meson::contract / Baryon::contract + fourier(FORWARD) on
+                      seeded propagators, lattice 4x2x4x4
+
+    python tests/golden/make_golden.py smear      (only ref_smear.npz)
+    python tests/golden/make_golden.py contract   (only ref_contract.npz)
 """
 from __future__ import annotations
 
@@ -115,12 +119,39 @@ def make_smear():
     print("ref_smear.npz", os.path.getsize(os.path.join(HERE, "ref_smear.npz")), "bytes")
 
 
+def seeded_propagator(L, seed):
+    """[V, 4, 4, 3, 3, 2] from 12 Gaussian spinor fields of the oracle's generator."""
+    f = np.stack([O.spinor_gaussian(L, seed + k) for k in range(12)], axis=1)  # [V, 12, 4, 3, 2]
+    return np.ascontiguousarray(f.reshape(-1, 4, 3, 4, 3, 2).transpose(0, 3, 1, 4, 2, 5))
+
+
+CONTRACT = {"L": (4, 2, 4, 4), "seed1": 61, "seed2": 81, "Q_sq": 2, "x_src": (1, 0, 3, 2)}
+
+
+def make_contract():
+    c = CONTRACT
+    L = c["L"]
+    p1, p2 = seeded_propagator(L, c["seed1"]), seeded_propagator(L, c["seed2"])
+    d = {k: np.array(v) for k, v in c.items()}
+    d["in_checksum"] = np.concatenate([checksum(p1), checksum(p2)])
+    d["momenta"] = O.momenta(c["Q_sq"])
+    for op, name in enumerate(O.MESONS):
+        d[f"meson:{name}"] = O.ref_meson_2pt(L, p1, op, c["Q_sq"], c["x_src"])
+    for op, name in enumerate(O.BARYONS):
+        d[f"baryon:{name}"] = O.ref_baryon_2pt(L, p1, p2, op, c["Q_sq"], c["x_src"])
+    np.savez_compressed(os.path.join(HERE, "ref_contract.npz"), **d)
+    print("ref_contract.npz", os.path.getsize(os.path.join(HERE, "ref_contract.npz")), "bytes")
+
+
 def main():
     O.build(ref=True)
     if not O.ref_available():
         raise SystemExit("reference build missing (oracle/_ref/libqkxref.so)")
     if sys.argv[1:] == ["smear"]:
         make_smear()
+        return
+    if sys.argv[1:] == ["contract"]:
+        make_contract()
         return
 
     # --- small lattice, full outputs
@@ -184,6 +215,7 @@ def main():
     for f in ("ref_ops_small.npz", "ref_ops_probe.npz", "ref_cg.npz"):
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
     make_smear()
+    make_contract()
 
 
 if __name__ == "__main__":
