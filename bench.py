@@ -20,6 +20,18 @@ time slice 2*rank): weak scaling, no data-path collective; `value` is the
 max over ranks of the per-step device time.
 `--impl reference` times the reference's own CPU code (compiled from its
 sources, oracle/_ref) on the host cores instead.
+
+Other workloads (one JSON line each, same --steps/--warmup rules, 1 GPU):
+  --workload propagator  the smeared-source propagator of bin/test_invert_prop.cpp
+                         (APE 20 x 0.5, Gaussian 50 x 4.0 at source and sink, 12
+                         point sources, mixed solver to 1e-10) at 32^3x64
+  --workload uneven      four lattices 16^3x32 .. 32^3x64 with their own links
+                         (eps ~ U[0.2, 0.35]) and masses {0.0015, 0.004, 0.01},
+                         12 solves of 4 Gaussian sources, run concurrently
+  --workload ptc         the learned preconditioner at 32^3x64: 64 training solves,
+                         --ptc-steps Adam steps, then flexible GCR on the 12 point sources
+  --workload contract    the 10 meson and 4 nucleon two-point functions with 33
+                         momenta (Q^2 <= 4) from a 32^3x64 propagator in HBM
 """
 from __future__ import annotations
 
@@ -336,6 +348,287 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# --------------------------------------------------------------------------- other workloads
+def _common(args, metric, value, unit, higher, workload, extra):
+    line = {"metric": metric, "value": value, "unit": unit, "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": higher, "scaling": "weak", "vs_baseline": None,
+            "data": "synthetic (seeded links and sources)", "config": {"workload": workload}}
+    line.update(extra)
+    print(json.dumps(line), flush=True)
+
+
+def _events(Q, lat):
+    import torch
+    stream = torch.cuda.ExternalStream(lat.stream())
+    return stream, torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def _roofline(kernel, launches, ms, nbytes, traffic=None):
+    peak, src = measured_peak_hbm()
+    avg = ms / max(launches, 1)
+    per = nbytes / max(launches, 1)
+    ach = per / (avg * 1e-3) / 1e9 if launches else None
+    return {"kernel": kernel, "bound": "hbm", "achieved": ach, "peak": peak, "peak_source": src, "unit": "GB/s",
+            "frac": ach / peak if ach else None, "traffic": traffic, "launches": launches, "avg_launch_ms": avg,
+            "algorithmic_bytes_per_launch": per}
+
+
+def run_propagator(args):
+    import numpy as np
+    import torch
+    import qkxtm_mpi_b200 as Q
+    torch.cuda.set_device(0)
+    NS, AL, NA, AA = 50, 4.0, 20, 0.5
+    lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, boundaryT=-1))
+    lat.generate_gauge(EPS, SEED, Q.LINKS_AS_GIVEN)
+    U = Q.pinned_array((lat.V, 4, 3, 3, 2))
+    U[...] = lat.download_gauge()
+    lat.APE_smearing(U, NA, AA, download=False)  # smearing links from the links without the boundary sign
+    lat.load_gauge(U, Q.LINKS_APPLY_BC)
+    lat.tune(Q.PREC_HALF, NSRC)
+    nbytes = lat.V * 2304
+    dprop = Q.lib().qkx_device_alloc(lat.ctx, nbytes)
+    stream, e0, e1 = _events(Q, lat)
+
+    def step():
+        info = lat.propagator_dev(dprop, (0, 0, 0, 0), NS, AL, tol=TOL)
+        if not info.converged:
+            raise RuntimeError("propagator solve did not converge")
+        return info
+
+    for _ in range(args.warmup):
+        step()
+    lat.sync()
+    k0 = lat.kernel_launches()
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            info = step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = lat.kernel_launches() - k0
+    step_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    # the Gaussian smearing kernel alone: 12 fields, 10 full-lattice steps
+    fs = [lat.field(np.random.default_rng(k).standard_normal((lat.V, 4, 3, 2))) for k in range(NSRC)]
+    gs = [lat.field() for _ in range(NSRC)]
+    lat.Gaussian_smearing_dev(fs, gs, 1, AL)
+    lat.sync()
+    lat.profile_reset()
+    lat.profile(True)
+    lat.Gaussian_smearing_dev(fs, gs, 10, AL)
+    lat.sync()
+    n, ms, by = lat.profile_read()
+    lat.profile(False)
+    for f in fs + gs:
+        f.close()
+    # end to end: host links in, host propagator out
+    out = Q.pinned_array((lat.V, 4, 4, 3, 3, 2))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    n_e2e = max(1, min(args.steps, 2))
+    for _ in range(n_e2e):
+        lat.load_gauge(U, Q.LINKS_APPLY_BC)
+        lat.APE_smearing(U, NA, AA, download=False)
+        lat.propagator((0, 0, 0, 0), NS, AL, tol=TOL, out=out)
+    e2e_s = (time.perf_counter() - t0) / n_e2e
+    Q.lib().qkx_device_free(lat.ctx, dprop)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import cpu_baseline as CB
+        cpu = CB.propagator_sample(L, KAPPA, MU, EPS, SEED, NS, AL)
+    _common(args, "smeared-source propagator time (12 point sources, 32^3x64)", step_s, "s", False,
+            f"APE {NA}x{AA}, Gaussian {NS}x{AL} at source and sink, 12 point sources, mixed solver to {TOL:g}, "
+            f"32^3x64, kappa={KAPPA}, mu={MU}",
+            {"ms_per_step": step_s * 1e3, "dtype": "f64 smearing / f16-f32-f64 solver",
+             "iterations": info.iterations, "true_residual_max": info.true_residual,
+             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 2 * U.nbytes,
+                     "d2h_bytes_per_step": out.nbytes},
+             "gpu_launches": launches,
+             "roofline": _roofline("k_gauss_step (12 fields, FP64, 18-real links)", n, ms, by),
+             "clocks": clk.summary(), **({"cpu_baseline": cpu} if cpu else {})})
+
+
+def run_uneven(args):
+    import numpy as np
+    import torch
+    import qkxtm_mpi_b200 as Q
+    torch.cuda.set_device(0)
+    lattices = [(16, 16, 16, 32), (20, 20, 20, 40), (24, 24, 24, 48), (32, 32, 32, 64)]
+    masses = [0.0015, 0.004, 0.01]
+    rng = np.random.default_rng(SEED)
+    lats, jobs, fields = [], [], []
+    for i, Li in enumerate(lattices):
+        eps = float(rng.uniform(0.2, 0.35))
+        lat = Q.Lattice(Q.LatticeInfo(L=Li, kappa=KAPPA, mu=MU, boundaryT=-1))
+        lat.generate_gauge(eps, SEED + i, Q.LINKS_APPLY_BC)
+        lat.tune(Q.PREC_HALF, 4)
+        lats.append((lat, eps))
+        for j in range(3):
+            bs = [lat.field(np.random.default_rng(1000 * i + 10 * j + k).standard_normal((lat.V, 4, 3, 2)))
+                  for k in range(4)]
+            xs = [lat.field() for _ in range(4)]
+            fields += bs + xs
+            jobs.append((lat, bs, xs, [masses[(j + k) % 3] for k in range(4)]))
+    for _ in range(args.warmup):
+        Q.invert_batch(jobs, tol=TOL)
+    lats_k0 = sum(l.kernel_launches() for l, _ in lats)
+    lat_all, steps_s = [], []
+    with ClockSampler(0) as clk:
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            res = Q.invert_batch(jobs, tol=TOL)
+            torch.cuda.synchronize()
+            steps_s.append(time.perf_counter() - t0)
+            lat_all += [r["latency"] for r in res]
+            if not all(r["info"]["converged"] for r in res):
+                raise RuntimeError("a batched solve did not converge")
+    launches = sum(l.kernel_launches() for l, _ in lats) - lats_k0
+    step_s = statistics.median(steps_s)
+    nrhs = 4 * len(jobs)
+    p50, p99 = float(np.percentile(lat_all, 50)), float(np.percentile(lat_all, 99))
+    # end to end: sources from pinned host memory, solutions back
+    hb = [Q.pinned_array((l.V, 4, 3, 2)) for (l, bs, xs, m) in jobs for _ in bs]
+    for i, h in enumerate(hb):
+        h[...] = np.random.default_rng(7000 + i).standard_normal(h.shape)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    k = 0
+    for (l, bs, xs, m) in jobs:
+        for b in bs:
+            Q.check(Q.lib().qkx_spinor_upload(l.ctx, hb[k].ctypes.data, b.ptr))
+            k += 1
+    Q.invert_batch(jobs, tol=TOL)
+    k = 0
+    for (l, bs, xs, m) in jobs:
+        for x in xs:
+            Q.check(Q.lib().qkx_spinor_download(l.ctx, x.ptr, hb[k].ctypes.data))
+            k += 1
+    e2e_s = time.perf_counter() - t0
+    nb = sum(h.nbytes for h in hb)
+    for f in fields:
+        f.close()
+    _common(args, "batched uneven solves: right-hand sides per second (4 lattices, 12 solves x 4 RHS)",
+            nrhs / step_s, "rhs/s", True,
+            "16^3x32, 20^3x40, 24^3x48, 32^3x64 with eps ~ U[0.2,0.35]; 3 solves x 4 Gaussian RHS each, "
+            "mu in {0.0015, 0.004, 0.01}; even-odd mixed CG to 1e-10; lattices concurrent on one GPU",
+            {"ms_per_step": step_s * 1e3, "dtype": "f16 storage / f32 accumulate / f64 reliable",
+             "latency_p50_s": p50, "latency_p99_s": p99, "batch_seconds": step_s,
+             "eps": [e for _, e in lats],
+             "e2e": {"value": nrhs / e2e_s, "unit": "rhs/s", "h2d_bytes_per_step": nb, "d2h_bytes_per_step": nb},
+             "gpu_launches": launches, "clocks": clk.summary()})
+
+
+def run_ptc(args):
+    import numpy as np
+    import torch
+    import qkxtm_mpi_b200 as Q
+    torch.cuda.set_device(0)
+    lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, boundaryT=-1))
+    lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
+    lat.tune(Q.PREC_HALF, NSRC)
+    net = Q.Ptc(lat, (4, 16, 16, 16, 4), seed=3, init_scale=0.05, tensor_cores=True)
+    train = net.train(n_solves=64, steps=args.ptc_steps, lr=3e-3, solve_tol=1e-6, seed=9)
+    srcs = point_sources(np, 0)
+    bd = [lat.field(b) for b in srcs]
+    xd = [lat.field() for _ in srcs]
+
+    def solve(pre):
+        return lat.invert_dev(bd, xd, method=Q.SOLVER_GCR_PTC, tol=TOL, preconditioner=pre)
+
+    for _ in range(args.warmup):
+        solve(net)
+    stream, e0, e1 = _events(Q, lat)
+    k0 = lat.kernel_launches()
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            info = solve(net)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = lat.kernel_launches() - k0
+    step_s = e0.elapsed_time(e1) / 1e3 / args.steps
+    plain_gcr = solve(None)
+    mixed = lat.invert_dev(bd, xd, method=Q.SOLVER_CG_EO_MIXED, tol=TOL)
+    fp64 = lat.invert_dev(bd, xd, method=Q.SOLVER_CG_FP64, tol=TOL, maxIter=5000)
+    # end to end from host buffers
+    bh = [Q.pinned_array((lat.V, 4, 3, 2)) for _ in srcs]
+    for h, b in zip(bh, srcs):
+        h[...] = b
+    xh = [Q.pinned_array((lat.V, 4, 3, 2)) for _ in srcs]
+    t0 = time.perf_counter()
+    lat.invert(bh, method=Q.SOLVER_GCR_PTC, tol=TOL, out=xh, preconditioner=net)
+    e2e_s = time.perf_counter() - t0
+    for f in bd + xd:
+        f.close()
+    net.close()
+    _common(args, "learned-preconditioned GCR time-to-solution at 1e-10, 12 point sources, 32^3x64", step_s, "s",
+            False, f"PTC 4 layers 4-16-16-16-4 channels, BF16 weights, tcgen05 16->16 layers; 64 training solves, "
+                   f"{args.ptc_steps} Adam steps; flexible GCR(16), FP64 defect correction; kappa={KAPPA}, mu={MU}",
+            {"ms_per_step": step_s * 1e3, "dtype": "bf16 network / f32 GCR / f64 residual",
+             "iterations": info.iterations, "fallbacks": info.fallbacks, "true_residual_max": info.true_residual,
+             "training": train,
+             "compare": {"gcr_no_preconditioner": {"seconds": plain_gcr.seconds, "iterations": plain_gcr.iterations,
+                                                   "fallbacks": plain_gcr.fallbacks},
+                         "mixed_cg": {"seconds": mixed.seconds, "iterations": mixed.iterations},
+                         "plain_fp64_cg": {"seconds": fp64.seconds, "iterations": fp64.iterations}},
+             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": sum(b.nbytes for b in bh),
+                     "d2h_bytes_per_step": sum(x.nbytes for x in xh)},
+             "gpu_launches": launches, "clocks": clk.summary()})
+
+
+def run_contract(args):
+    import numpy as np
+    import torch
+    import qkxtm_mpi_b200 as Q
+    torch.cuda.set_device(0)
+    Qsq = 4
+    lat = Q.Lattice(Q.LatticeInfo(L=L))
+    V = lat.V
+    host = Q.pinned_array((V, 4, 4, 3, 3, 2))
+    host[...] = np.random.default_rng(SEED).standard_normal(host.shape)
+    nbytes = V * 2304
+    d = Q.lib().qkx_device_alloc(lat.ctx, nbytes)
+    Q.check(Q.lib().qkx_memcpy_h2d(lat.ctx, d, host.ctypes.data, nbytes))
+
+    def step():
+        lat.meson_2pt(d, range(10), Qsq, (0, 0, 0, 0), device=True)
+        for op in range(4):
+            lat.baryon_2pt(d, d, op, Qsq, (0, 0, 0, 0), device=True)
+
+    for _ in range(args.warmup):
+        step()
+    k0 = lat.kernel_launches()
+    with ClockSampler(0) as clk:
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            step()
+        torch.cuda.synchronize()
+        step_s = (time.perf_counter() - t0) / args.steps
+    launches = lat.kernel_launches() - k0
+    t0 = time.perf_counter()
+    lat.meson_2pt(host, range(10), Qsq)
+    for op in range(4):
+        lat.baryon_2pt(host, host, op, Qsq)
+    e2e_s = time.perf_counter() - t0
+    Q.lib().qkx_device_free(lat.ctx, d)
+    cpu = None
+    if not args.no_cpu_baseline:
+        from oracle import cpu_baseline as CB
+        cpu = CB.contract_sample(L, Qsq)
+    nmom = len(Q.momenta(Qsq))
+    _common(args, "two-point functions per propagator: 10 mesons + 4 nucleon operators, 33 momenta, 32^3x64",
+            step_s, "s", False, f"Meson::contract x10 + Baryon::contract x4 + Fourier to {nmom} momenta "
+                                f"(Q^2 <= {Qsq}) from a 32^3x64 propagator in HBM",
+            {"ms_per_step": step_s * 1e3, "dtype": "f64",
+             "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": 9 * host.nbytes,
+                     "d2h_bytes_per_step": 8 * L[3] * nmom * (10 + 4 * 16) * 2},
+             "gpu_launches": launches, "clocks": clk.summary(), **({"cpu_baseline": cpu} if cpu else {})})
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
@@ -345,14 +638,23 @@ def main():
     ap.add_argument("--precision", choices=["half", "single", "double"], default="half")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--workload", choices=["cg", "propagator", "uneven", "ptc", "contract"], default="cg")
+    ap.add_argument("--ptc-steps", type=int, default=2000)
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: --warmup below 3 raised to 3", file=sys.stderr)
         args.warmup = 3
     if args.impl == "reference":
+        if args.workload != "cg":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference arm is defined for the default "
+                              "workload; the other workloads carry their own cpu_baseline"}), flush=True)
+            return
         run_reference(args)
-    else:
+    elif args.workload == "cg":
         run_ours(args)
+    else:
+        {"propagator": run_propagator, "uneven": run_uneven, "ptc": run_ptc, "contract": run_contract}[
+            args.workload](args)
 
 
 if __name__ == "__main__":

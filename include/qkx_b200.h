@@ -244,6 +244,25 @@ QKX_API int qkx_invert(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, cons
 QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, const double* const* b_dev,
                    double* const* x_dev, qkx_solve_info* info);
 
+/* Many solves on several lattices at once (no reference counterpart).  Each
+ * job is one qkx_invert_dev on its context (a lattice with its own links,
+ * parameters and stream).  The jobs of a context run in order on one host
+ * thread, different contexts on different threads, so their kernels overlap
+ * on the GPU; contexts start in order of decreasing volume.  sp applies to
+ * every job (its mu replaced by the job's). */
+typedef struct qkx_batch_job {
+  qkx_ctx* ctx;                /* the job's lattice */
+  int nrhs;                    /* right-hand sides of this job */
+  const double* const* b_dev;  /* nrhs device fields in the context's even-odd layout */
+  double* const* x_dev;        /* nrhs device fields for the solutions */
+  const double* mu;            /* NULL, or nrhs twisted masses */
+  int status;                  /* out: QKX_OK or the job's error code */
+  double latency;              /* out: seconds from the start of the batch to this job's results */
+  qkx_solve_info info;         /* out */
+  char message[160];           /* out: the error message when status != QKX_OK */
+} qkx_batch_job;
+QKX_API int qkx_invert_batch(qkx_batch_job* jobs, int njobs, const qkx_solver_params* sp);
+
 /* Autotune the inner hop of CG_EO_MIXED for this lattice, precision and batch
  * size: times every tile (right-hand sides per thread x threads per block) on
  * the device and keeps the fastest for later solves (a solve with an untuned

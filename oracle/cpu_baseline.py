@@ -115,6 +115,52 @@ def run(L, kappa, mu, eps, seed, n_sources=12, n_iter=1, procs=None, iters_full=
             "iters_full": iters_full}
 
 
+def propagator_sample(L, kappa, mu, eps, seed, nsmear, alpha, n_sources=12, small=(16, 16, 16, 32)) -> dict:
+    """The reference's smeared-source propagator loop (bin/test_invert_prop.cpp:83-97)
+    on the host: per source two Gaussian smearings of nsmear steps and one CG
+    solve.  The smearing is timed with the reference's Vector::Gaussian_smearing
+    (2 steps of one vector on `small`) and scaled by volume; the solves come from
+    run() (concurrent single-rank processes, as for the CG baseline)."""
+    O.build(ref=True)
+    kind = "reference" if O.ref_available() else "port"
+    U = O.gauge_random(small, eps, seed)
+    psi = O.spinor_gaussian(small, seed + 1)
+    smear = O.ref_gaussian_smear if kind == "reference" else O.gaussian_smear
+    t0 = time.perf_counter()
+    smear(small, U, psi, 2, alpha)
+    t_step = (time.perf_counter() - t0) / 2 * (O.volume(L) / O.volume(small))
+    cg = run(L, kappa, mu, eps, seed, n_sources=n_sources, n_iter=1)
+    P = cg["cores"]
+    smear_total = math.ceil(n_sources / P) * 2 * nsmear * t_step
+    value = smear_total + cg["value"]
+    sample = (f"{kind} Gaussian_smearing, 2 steps of one vector on {'x'.join(map(str, small))} scaled by volume "
+              f"({t_step:.2f} s/step at full size) x 2 x {nsmear} steps per source; solves: {cg['sample']}")
+    return {"value": value, "unit": "s", "cores": P, "kind": kind, "sample": sample}
+
+
+def contract_sample(L, Q_sq, small=(8, 8, 8, 16)) -> dict:
+    """The reference's Meson::contract x10 and Baryon::contract x4 with their
+    Fourier transforms, timed on `small` (one process) and scaled by volume:
+    both the site contractions and the transform are linear in V."""
+    O.build(ref=True)
+    kind = "reference" if O.ref_available() else "port"
+    V = O.volume(small)
+    rng = np.random.default_rng(1)
+    p = rng.standard_normal((V, 4, 4, 3, 3, 2))
+    meson = O.ref_meson_2pt if kind == "reference" else O.meson_2pt
+    baryon = O.ref_baryon_2pt if kind == "reference" else O.baryon_2pt
+    t0 = time.perf_counter()
+    for op in range(10):
+        meson(small, p, op, Q_sq)
+    for op in range(4):
+        baryon(small, p, p, op, Q_sq)
+    t = time.perf_counter() - t0
+    value = t * O.volume(L) / V
+    sample = (f"{kind} contractions (10 mesons + 4 nucleon operators, Q^2 <= {Q_sq}) on "
+              f"{'x'.join(map(str, small))} in {t:.2f} s, scaled by volume to {'x'.join(map(str, L))}")
+    return {"value": value, "unit": "s", "cores": 1, "kind": kind, "sample": sample}
+
+
 if __name__ == "__main__":
     # worker process: time n_iter CG iterations and print the seconds
     print(_worker(json.loads(sys.argv[1])), flush=True)

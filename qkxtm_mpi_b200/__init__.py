@@ -73,7 +73,7 @@ SYMBOLS = [
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
     "qkx_ptc_set_weights", "qkx_ptc_apply", "qkx_ptc_loss_grad", "qkx_ptc_train",
     "qkx_read_gauge_lime", "qkx_write_gauge_lime", "qkx_momenta", "qkx_meson_2pt", "qkx_meson_2pt_dev",
-    "qkx_baryon_2pt", "qkx_baryon_2pt_dev",
+    "qkx_baryon_2pt", "qkx_baryon_2pt_dev", "qkx_invert_batch",
 ]
 
 
@@ -128,6 +128,12 @@ class SolveInfo(C.Structure):
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+class BatchJob(C.Structure):
+    _fields_ = [("ctx", C.c_void_p), ("nrhs", C.c_int), ("b_dev", C.POINTER(C.c_void_p)),
+                ("x_dev", C.POINTER(C.c_void_p)), ("mu", C.POINTER(C.c_double)), ("status", C.c_int),
+                ("latency", C.c_double), ("info", SolveInfo), ("message", C.c_char * 160)]
 
 
 _lib = None
@@ -214,6 +220,7 @@ def lib() -> C.CDLL:
         L.qkx_ptc_train.argtypes = [_vp, C.POINTER(PtcTrainParams), C.POINTER(PtcTrainInfo)]
         L.qkx_read_gauge_lime.argtypes = [_vp, C.c_char_p, C.c_int, _vp, C.POINTER(LimeInfo)]
         L.qkx_write_gauge_lime.argtypes = [_vp, C.c_char_p, _vp, C.c_char_p]
+        L.qkx_invert_batch.argtypes = [C.POINTER(BatchJob), C.c_int, C.POINTER(SolverParams)]
         L.qkx_momenta.argtypes = [C.c_int, _vp, C.c_int]
         L.qkx_meson_2pt.argtypes = [_vp, _vp, C.c_int, _vp, C.c_int, C.POINTER(C.c_int), _vp]
         L.qkx_meson_2pt_dev.argtypes = L.qkx_meson_2pt.argtypes
@@ -480,9 +487,13 @@ class Lattice:
         return U
 
     def APE_smearing(self, U_in: np.ndarray, nsmear: int = 20, alpha: float = 0.5,
-                     out: np.ndarray | None = None) -> np.ndarray | None:
+                     out: np.ndarray | None = None, download: bool = True) -> np.ndarray | None:
         """Gauge::APE_smearing of U_in; the result also becomes the smearing links.
-        Returns the smeared field (out, or a new array); nsmear == 0 leaves out as it was."""
+        Returns the smeared field (out, or a new array; None with download=False);
+        nsmear == 0 leaves out as it was."""
+        if not download:
+            check(lib().qkx_ape_smear(self.ctx, _host(U_in).ctypes.data, None, nsmear, alpha))
+            return None
         out = np.zeros_like(_host(U_in)) if out is None else out
         check(lib().qkx_ape_smear(self.ctx, _host(U_in).ctypes.data, out.ctypes.data, nsmear, alpha))
         return out
@@ -644,6 +655,29 @@ class Ptc:
         info = PtcTrainInfo()
         check(lib().qkx_ptc_train(self.ptr, C.byref(tp), C.byref(info)))
         return info.as_dict()
+
+
+def invert_batch(jobs, method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_HALF, tol: float = 1e-10,
+                 maxIter: int = 10000, use_graphs: int = 1):
+    """Run many solves on several lattices concurrently (qkx_invert_batch).
+    jobs: list of (Lattice, [DeviceField b], [DeviceField x], mu list or None).
+    Returns a list of dicts with the status, latency (s from the batch start) and solve info."""
+    arr = (BatchJob * len(jobs))()
+    keep = []
+    for j, (lat, bs, xs, mus) in zip(arr, jobs):
+        bp = (_vp * len(bs))(*[b.ptr for b in bs])
+        xp = (_vp * len(xs))(*[x.ptr for x in xs])
+        mp = (C.c_double * len(mus))(*mus) if mus is not None else None
+        keep += [bp, xp, mp]
+        j.ctx, j.nrhs, j.b_dev, j.x_dev = lat.ctx, len(bs), bp, xp
+        j.mu = C.cast(mp, C.POINTER(C.c_double)) if mp is not None else None
+    sp = SolverParams(method, precision, tol, maxIter, 0.0, use_graphs, None, None)
+    rc = lib().qkx_invert_batch(arr, len(jobs), C.byref(sp))
+    out = [{"status": j.status, "latency": j.latency, "info": j.info.as_dict(), "message": j.message.decode()}
+           for j in arr]
+    if rc != OK:
+        check(rc)
+    return out
 
 
 MESONS = ["ONE", "G5", "G1", "G2", "G3", "G4", "G5G1", "G5G2", "G5G3", "G5G4"]

@@ -29,6 +29,8 @@ namespace qkx {
 namespace {
 
 constexpr int CT_SITES = 16;           // sites per block
+constexpr int CT_STRIDE = 145;         // double2 per staged site: 144 + 1 of padding, so the 16 sites
+                                       // of a warp fall on different shared-memory banks
 constexpr double REF_PI = 3.14159265359;
 using zc = std::complex<double>;
 
@@ -164,27 +166,28 @@ __device__ __forceinline__ double2 cm(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// stage CT_SITES site blocks (144 complex each) of a propagator into shared memory
+// stage CT_SITES site blocks (144 complex each) of a propagator into shared
+// memory, site s at sp + s * CT_STRIDE
 __device__ __forceinline__ void stage(double2* sp, const double2* __restrict__ prop, size_t s0, size_t V) {
   const size_t base = s0 * 144;
-  const size_t total = (size_t)CT_SITES * 144;
-  for (size_t i = threadIdx.x; i < total; i += blockDim.x) {
+  const int total = CT_SITES * 144;
+  for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const size_t site = s0 + i / 144;
-    sp[i] = site < V ? __ldg(prop + base + i) : make_double2(0.0, 0.0);
+    sp[(i / 144) * CT_STRIDE + i % 144] = site < V ? __ldg(prop + base + i) : make_double2(0.0, 0.0);
   }
 }
 
 // C[op][site], block = CT_SITES sites x nop operators
 __global__ void k_meson_sites(const double2* __restrict__ prop, size_t V, int nop, const MesonTerms* __restrict__ T,
                               double2* __restrict__ C) {
-  __shared__ double2 sp[CT_SITES * 144];
+  __shared__ double2 sp[CT_SITES * CT_STRIDE];
   const size_t s0 = (size_t)blockIdx.x * CT_SITES;
   stage(sp, prop, s0, V);
   __syncthreads();
   const int ls = threadIdx.x % CT_SITES, o = threadIdx.x / CT_SITES;
   const size_t site = s0 + ls;
   if (o >= nop || site >= V) return;
-  const double2* pp = sp + ls * 144;  // [mu][nu][c1][c2] at mu*36 + nu*9 + c1*3 + c2
+  const double2* pp = sp + ls * CT_STRIDE;  // [mu][nu][c1][c2] at mu*36 + nu*9 + c1*3 + c2
   const MesonTerms& t = T[o];
   double2 m = make_double2(0.0, 0.0);
   for (int a = 0; a < 3; a++)
@@ -200,8 +203,10 @@ __global__ void k_meson_sites(const double2* __restrict__ prop, size_t V, int no
   C[(size_t)o * V + site] = m;
 }
 
-__constant__ int c_eps[6][3] = {{0, 1, 2}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
-__constant__ int c_sgn[6] = {+1, +1, +1, -1, -1, -1};
+// the even then odd permutations of (0, 1, 2) and their signs, in the reference's order
+// (lib/contractions.cpp:21-33)
+__device__ constexpr int c_eps[6][3] = {{0, 1, 2}, {2, 0, 1}, {1, 2, 0}, {2, 1, 0}, {0, 2, 1}, {1, 0, 2}};
+__device__ constexpr int c_sgn[6] = {+1, +1, +1, -1, -1, -1};
 
 // C[gamma*4 + gamma'][site], block = CT_SITES sites x 16 spin pairs
 __global__ void __launch_bounds__(CT_SITES * 16) k_baryon_sites(const double2* __restrict__ p1,
@@ -210,7 +215,7 @@ __global__ void __launch_bounds__(CT_SITES * 16) k_baryon_sites(const double2* _
                                                                 double2* __restrict__ C) {
   extern __shared__ double2 sb[];
   double2* s1 = sb;
-  double2* s2 = sb + CT_SITES * 144;
+  double2* s2 = sb + CT_SITES * CT_STRIDE;
   const size_t s0 = (size_t)blockIdx.x * CT_SITES;
   stage(s1, p1, s0, V);
   stage(s2, p2, s0, V);
@@ -218,23 +223,35 @@ __global__ void __launch_bounds__(CT_SITES * 16) k_baryon_sites(const double2* _
   const int ls = threadIdx.x % CT_SITES, k = threadIdx.x / CT_SITES;
   const size_t site = s0 + ls;
   if (site >= V) return;
-  const double2* q1 = s1 + ls * 144;
-  const double2* q2 = s2 + ls * 144;
+  const double2* q1 = s1 + ls * CT_STRIDE;
+  const double2* q2 = s2 + ls * CT_STRIDE;
   double2 m = make_double2(0.0, 0.0);
   const int n = T->n[k];
   for (int i = 0; i < n; i++) {
     const double2 val = T->val[k][i];
     const char4 ab = T->ab[k][i];  // alpha, beta, beta', alpha'
     const char2 xy = T->xy[k][i];
+    // the five colour matrices of the term, read once
+    double2 A[9], B[9], Cm[9], D[9], E[9];
+#pragma unroll
+    for (int u = 0; u < 9; u++) {
+      A[u] = q1[ab.x * 36 + ab.w * 9 + u];   // P1[alpha][alpha']
+      B[u] = q1[xy.x * 36 + xy.y * 9 + u];   // P1[X][Y]
+      Cm[u] = q1[ab.x * 36 + xy.y * 9 + u];  // P1[alpha][Y]
+      D[u] = q1[xy.x * 36 + ab.w * 9 + u];   // P1[X][alpha']
+      E[u] = q2[ab.y * 36 + ab.z * 9 + u];   // P2[beta][beta']
+    }
+#pragma unroll
     for (int e1 = 0; e1 < 6; e1++) {
       const int a = c_eps[e1][0], b = c_eps[e1][1], c = c_eps[e1][2];
+#pragma unroll
       for (int e2 = 0; e2 < 6; e2++) {
         const int a1 = c_eps[e2][0], b1 = c_eps[e2][1], c1 = c_eps[e2][2];
         const double f = (double)(c_sgn[e1] * c_sgn[e2]);
         const double2 fv = make_double2(f * val.x, f * val.y);
-        const double2 x1 = cm(q1[ab.x * 36 + ab.w * 9 + a * 3 + a1], q1[xy.x * 36 + xy.y * 9 + c * 3 + c1]);
-        const double2 x2 = cm(q1[ab.x * 36 + xy.y * 9 + a * 3 + c1], q1[xy.x * 36 + ab.w * 9 + c * 3 + a1]);
-        const double2 t = cm(cm(fv, q2[ab.y * 36 + ab.z * 9 + b * 3 + b1]), make_double2(x1.x - x2.x, x1.y - x2.y));
+        const double2 x1 = cm(A[a * 3 + a1], B[c * 3 + c1]);
+        const double2 x2 = cm(Cm[a * 3 + c1], D[c * 3 + a1]);
+        const double2 t = cm(cm(fv, E[b * 3 + b1]), make_double2(x1.x - x2.x, x1.y - x2.y));
         m.x += sign * t.x;
         m.y += sign * t.y;
       }
@@ -383,7 +400,7 @@ int baryon_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op
   QKX_CUDA(cudaMallocAsync((void**)&C, sizeof(double2) * 16 * c->V, c->st));
   QKX_CUDA(cudaMemcpyAsync(dT, &T, sizeof(BaryonTerms), cudaMemcpyHostToDevice, c->st));
   static bool attr = false;
-  const int smem = (int)(sizeof(double2) * 2 * CT_SITES * 144);
+  const int smem = (int)(sizeof(double2) * 2 * CT_SITES * CT_STRIDE);
   if (!attr) {
     QKX_CUDA(cudaFuncSetAttribute(k_baryon_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     attr = true;
