@@ -20,6 +20,7 @@
 #define QKXTM_B200_HPP
 
 #include <complex>
+#include <cstdio>
 #include <cstring>
 #include <memory>
 #include <stdexcept>
@@ -238,6 +239,9 @@ class Gauge {
     check(qkx_set_params(ctx_->c, &p));
     return ctx_->c;
   }
+  const LatticeInfo& info() const { return info_; }
+  // M was written outside the class: upload it again before the next use
+  void mark_modified() { dirty_ = smear_dirty_ = true; }
 
  private:
   LatticeInfo info_;
@@ -387,6 +391,69 @@ class Propagator {
   LatticeInfo info_;
   std::vector<Complex> storage_;
 };
+
+// ---- ILDG configurations (lib/read_conf_lime.cpp:111, lib/write_conf_lime.cpp:49)
+// qkxTM_MPI_getGaugeLime: fill u.M from an ILDG file (read and byte-swapped on the GPU).
+inline int qkxTM_MPI_getGaugeLime(char* fname, Gauge& u) {
+  check(qkx_read_gauge_lime(detail::plain_ctx(u.info()), fname, QKX_LINKS_AS_GIVEN, u.data(), nullptr));
+  u.mark_modified();
+  return 0;
+}
+// qkxTM_writeGaugeLime: write u.M as an ILDG file with message as its xlf-info record.
+inline int qkxTM_writeGaugeLime(char* fname, Gauge& u, char* message) {
+  check(qkx_write_gauge_lime(detail::plain_ctx(u.info()), fname, u.data(), message));
+  return 0;
+}
+
+// ---- two-point functions (lib/contractions.cpp:873-914), on the GPU, written
+// in the reference's text format (Meson::dumpData :149, Baryon::dumpData :641)
+inline void contractMesons(Propagator* prop1, Propagator* prop2, char* twop_filename, LatticeInfo* latInfo) {
+  qkx_ctx* c = detail::plain_ctx(*latInfo);
+  const int nmom = qkx_momenta(latInfo->Q_sq, nullptr, 0);
+  std::vector<int> mom((size_t)3 * nmom);
+  qkx_momenta(latInfo->Q_sq, mom.data(), nmom);
+  const int ops[QKX_NUM_MESONS] = {0, 1, 2, 3, 4, 5, 6, 7, 8, 9};
+  const int Lt = latInfo->L[3];
+  std::vector<double> F((size_t)QKX_NUM_MESONS * Lt * nmom * 2);
+  FILE* f = std::fopen(twop_filename, "w");
+  if (!f) throw Error(QKX_ERR_INVALID, "qkx_b200: cannot open the meson output file");
+  for (Propagator* p : {prop1, prop2}) {
+    check(qkx_meson_2pt(c, p->data(), QKX_NUM_MESONS, ops, latInfo->Q_sq, latInfo->x_src, F.data()));
+    for (int op = 0; op < QKX_NUM_MESONS; op++)
+      for (int t = 0; t < Lt; t++)
+        for (int im = 0; im < nmom; im++) {
+          const double* v = &F[(((size_t)op * Lt + t) * nmom + im) * 2];
+          std::fprintf(f, "%d \t %d \t %+d %+d %+d \t %+e %+e\n", op, t, mom[3 * im], mom[3 * im + 1],
+                       mom[3 * im + 2], v[0], v[1]);
+        }
+  }
+  std::fclose(f);
+}
+
+inline void contractBaryons(Propagator* prop1, Propagator* prop2, char* twop_filename, LatticeInfo* latInfo) {
+  qkx_ctx* c = detail::plain_ctx(*latInfo);
+  const int nmom = qkx_momenta(latInfo->Q_sq, nullptr, 0);
+  std::vector<int> mom((size_t)3 * nmom);
+  qkx_momenta(latInfo->Q_sq, mom.data(), nmom);
+  const int Lt = latInfo->L[3];
+  std::vector<double> F((size_t)Lt * nmom * 16 * 2);
+  FILE* f = std::fopen(twop_filename, "w");
+  if (!f) throw Error(QKX_ERR_INVALID, "qkx_b200: cannot open the baryon output file");
+  Propagator* pairs[2][2] = {{prop1, prop2}, {prop2, prop1}};
+  for (auto& pr : pairs)
+    for (int op = 0; op < 4; op++) {
+      check(qkx_baryon_2pt(c, pr[0]->data(), pr[1]->data(), op, latInfo->Q_sq, latInfo->x_src, F.data()));
+      for (int t = 0; t < Lt; t++)
+        for (int im = 0; im < nmom; im++)
+          for (int g = 0; g < 4; g++)
+            for (int gp = 0; gp < 4; gp++) {
+              const double* v = &F[((((size_t)t * nmom + im) * 4 + g) * 4 + gp) * 2];
+              std::fprintf(f, "%d \t %d \t %+d %+d %+d \t %d %d \t %+e %+e\n", op, t, mom[3 * im],
+                           mom[3 * im + 1], mom[3 * im + 2], g, gp, v[0], v[1]);
+            }
+    }
+  std::fclose(f);
+}
 
 // ---- class CG (include/solvers.h:3-22, lib/solvers.cpp)
 class CG {

@@ -2,8 +2,11 @@
 // bin/test_invert.cpp, bin/test_invert_prop.cpp) written against
 // include/qkxTM_b200.hpp, checked against the CPU oracle.  Built and run by
 // tests/test_gpu_dropin.py.
+#include <unistd.h>
+
 #include <cmath>
 #include <cstdio>
+#include <string>
 
 #include "../../include/qkxTM_b200.hpp"
 #include "../../oracle/qkx_oracle.h"
@@ -162,6 +165,56 @@ int main() {
     e = rel(prop2.data(), prop.data(), 288 * Vs);
     printf("propagator    batched vs loop rel err %.2e (true residual %.2e)\n", e, pi.true_residual);
     fails += e > 1e-8;
+
+    // ILDG round trip (lib/write_conf_lime.cpp, lib/read_conf_lime.cpp) and the
+    // contraction drivers (lib/contractions.cpp:873-914)
+    std::string tag = "/tmp/qkx_dropin_" + std::to_string(getpid());
+    std::string conf = tag + ".lime", twop = tag + "_mesons.dat", twob = tag + "_baryons.dat";
+    char msg[] = "drop-in test";
+    qkxTM_writeGaugeLime(&conf[0], *g, msg);
+    Gauge* g2 = new Gauge(&li);
+    qkxTM_MPI_getGaugeLime(&conf[0], *g2);
+    const bool same = std::memcmp(g2->data(), g->data(), sizeof(double) * 72 * Vs) == 0;
+    printf("ILDG          write + read %s\n", same ? "identical" : "DIFFERENT");
+    fails += !same;
+    li.Q_sq = 1;
+    contractMesons(&prop, &prop2, &twop[0], &li);
+    contractBaryons(&prop, &prop2, &twob[0], &li);
+    int mom[7 * 3];
+    const int nmom = orc_momenta(1, mom, 7);
+    std::vector<double> cref((size_t)2 * li.L[3] * nmom), bref((size_t)32 * li.L[3] * nmom);
+    orc_meson_2pt(li.L, prop.data(), 0, 1, li.x_src, cref.data());
+    orc_baryon_2pt(li.L, prop2.data(), prop.data(), 3, 1, li.x_src, bref.data());
+    // line 0: ONE of prop, t = 0, first momentum; the baryon file's last block: RTR of (prop2, prop)
+    FILE* fm = fopen(twop.c_str(), "r");
+    int op, t, n0, n1, n2;
+    double re = 0, im = 0;
+    int lines = 0, ok_line = fscanf(fm, "%d %d %d %d %d %lf %lf", &op, &t, &n0, &n1, &n2, &re, &im) == 7;
+    fseek(fm, 0, SEEK_SET);
+    for (int ch; (ch = fgetc(fm)) != EOF;) lines += ch == '\n';
+    fclose(fm);
+    double em = std::hypot(re - cref[0], im - cref[1]) / std::hypot(cref[0], cref[1]);
+    FILE* fb = fopen(twob.c_str(), "r");
+    int blines = 0, g0, g1;
+    double br = 0, bi = 0, eb = 0;
+    for (int k = 0; fscanf(fb, "%d %d %d %d %d %d %d %lf %lf", &op, &t, &n0, &n1, &n2, &g0, &g1, &br, &bi) == 9; k++) {
+      blines++;
+      if (k >= 7 * li.L[3] * nmom * 16) {  // the second propagator pair's RTR block
+        const int j = k - 7 * li.L[3] * nmom * 16;
+        eb = std::max(eb, std::hypot(br - bref[2 * j], bi - bref[2 * j + 1]));
+      }
+    }
+    fclose(fb);
+    double bmax = 0;
+    for (double v : bref) bmax = std::max(bmax, std::fabs(v));
+    printf("contractions  %d meson lines (rel err %.1e), %d baryon lines (max err %.1e of %.1e)\n", lines, em,
+           blines, eb, bmax);
+    fails += !ok_line || lines != 2 * 10 * li.L[3] * nmom || em > 1e-6;  // the text keeps 7 digits
+    fails += blines != 8 * li.L[3] * nmom * 16 || eb > 1e-6 * bmax;
+    unlink(conf.c_str());
+    unlink(twop.c_str());
+    unlink(twob.c_str());
+    delete g2;
     delete g_ape;
     delete g_tmp;
     delete g;
