@@ -32,6 +32,10 @@ Other workloads (one JSON line each, same --steps/--warmup rules, 1 GPU):
                          --ptc-steps Adam steps, then flexible GCR on the 12 point sources
   --workload contract    the 10 meson and 4 nucleon two-point functions with 33
                          momenta (Q^2 <= 4) from a 32^3x64 propagator in HBM
+  --workload dslash      the Dslash alone: the 12-RHS even-odd hop in FP16 and FP32
+                         (autotuned tile) and the FP64 full-lattice M, in GB/s
+--lattice X,Y,Z,T replaces 32^3x64 in the non-default workloads (small cases for
+profiling).
 """
 from __future__ import annotations
 
@@ -120,9 +124,10 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def point_sources(np, t_src: int):
-    V = L[0] * L[1] * L[2] * L[3]
-    site = L[0] * L[1] * L[2] * t_src
+def point_sources(np, t_src: int, Ls=None):
+    Ls = Ls or L
+    V = Ls[0] * Ls[1] * Ls[2] * Ls[3]
+    site = Ls[0] * Ls[1] * Ls[2] * t_src
     out = []
     for s in range(4):
         for c in range(3):
@@ -373,12 +378,61 @@ def _roofline(kernel, launches, ms, nbytes, traffic=None):
             "algorithmic_bytes_per_launch": per}
 
 
+def run_dslash(args):
+    import numpy as np
+    import torch
+    import qkxtm_mpi_b200 as Q
+    torch.cuda.set_device(0)
+    Lw = args.lattice
+    lat = Q.Lattice(Q.LatticeInfo(L=Lw, kappa=KAPPA, mu=MU, boundaryT=-1))
+    lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
+    Vh = lat.V // 2
+    hops = {}
+    with ClockSampler(0) as clk:
+        for name, prec, S, G in (("fp16", Q.PREC_HALF, 52.0, 24.0), ("fp32", Q.PREC_SINGLE, 96.0, 48.0)):
+            nr, nt, ms = lat.tune(prec, NSRC)  # CUDA events around 3 pairs of Schur hops per tile, best tile
+            # one output parity: input and output spinors, links shared by the batch, the
+            # xpay operand on every second hop of the pair
+            nbytes = Vh * NSRC * (2.5 * S + 8.0 * G / NSRC)
+            hops[name] = {"tile": [nr, nt], "ms_per_hop": ms, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                          "algorithmic_bytes_per_hop": nbytes}
+        a = lat.field(np.random.default_rng(1).standard_normal((lat.V, 4, 3, 2)))
+        b = lat.field()
+        for _ in range(args.warmup):
+            lat.apply_dev("tm", a, b)
+        lat.sync()
+        lat.profile_reset()
+        lat.profile(True)
+        for _ in range(args.steps):
+            lat.apply_dev("tm", a, b)
+        lat.sync()
+        n, ms, by = lat.profile_read()
+        lat.profile(False)
+    a.close()
+    b.close()
+    fp64 = {"launches": n, "ms": ms / max(n, 1), "gbs": by / (ms * 1e-3) / 1e9,
+            "gflops": 1416.0 * lat.V * n / (ms * 1e-3) / 1e9}
+    peak, src = measured_peak_hbm()
+    lat_s = "x".join(map(str, Lw))
+    _common(args, f"Dslash HBM GB/s: even-odd hop, {NSRC} RHS, FP16 spinors and 12-real links, {lat_s}",
+            hops["fp16"]["gbs"], "GB/s", True,
+            f"hop_mrhs_kernel on one parity of {lat_s} for a batch of {NSRC} right-hand sides (autotuned tile), "
+            f"kappa={KAPPA}, mu={MU}; FP64 full-lattice M beside it",
+            {"dtype": "f16 storage / f32 arithmetic", "fp32": hops["fp32"], "fp64_tm": fp64,
+             "roofline": {"kernel": "hop_mrhs_kernel<fp16>", "bound": "hbm", "achieved": hops["fp16"]["gbs"],
+                          "peak": peak, "peak_source": src, "unit": "GB/s", "frac": hops["fp16"]["gbs"] / peak,
+                          "traffic": None, "algorithmic_bytes_per_launch": hops["fp16"]["algorithmic_bytes_per_hop"],
+                          "avg_launch_ms": hops["fp16"]["ms_per_hop"]},
+             "gpu_launches": lat.kernel_launches(), "clocks": clk.summary()})
+
+
 def run_propagator(args):
     import numpy as np
     import torch
     import qkxtm_mpi_b200 as Q
     torch.cuda.set_device(0)
     NS, AL, NA, AA = 50, 4.0, 20, 0.5
+    L = args.lattice
     lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, boundaryT=-1))
     lat.generate_gauge(EPS, SEED, Q.LINKS_AS_GIVEN)
     U = Q.pinned_array((lat.V, 4, 3, 3, 2))
@@ -525,12 +579,13 @@ def run_ptc(args):
     import torch
     import qkxtm_mpi_b200 as Q
     torch.cuda.set_device(0)
+    L = args.lattice
     lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, boundaryT=-1))
     lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
     lat.tune(Q.PREC_HALF, NSRC)
     net = Q.Ptc(lat, (4, 16, 16, 16, 4), seed=3, init_scale=0.05, tensor_cores=True)
     train = net.train(n_solves=64, steps=args.ptc_steps, lr=3e-3, solve_tol=1e-6, seed=9)
-    srcs = point_sources(np, 0)
+    srcs = point_sources(np, 0, L)
     bd = [lat.field(b) for b in srcs]
     xd = [lat.field() for _ in srcs]
 
@@ -584,6 +639,7 @@ def run_contract(args):
     import torch
     import qkxtm_mpi_b200 as Q
     torch.cuda.set_device(0)
+    L = args.lattice
     Qsq = 4
     lat = Q.Lattice(Q.LatticeInfo(L=L))
     V = lat.V
@@ -638,8 +694,11 @@ def main():
     ap.add_argument("--precision", choices=["half", "single", "double"], default="half")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
-    ap.add_argument("--workload", choices=["cg", "propagator", "uneven", "ptc", "contract"], default="cg")
+    ap.add_argument("--workload", choices=["cg", "propagator", "uneven", "ptc", "contract", "dslash"],
+                    default="cg")
     ap.add_argument("--ptc-steps", type=int, default=2000)
+    ap.add_argument("--lattice", type=lambda v: tuple(int(x) for x in v.split(",")), default=L,
+                    help="X,Y,Z,T for the non-default workloads")
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: --warmup below 3 raised to 3", file=sys.stderr)
@@ -653,8 +712,8 @@ def main():
     elif args.workload == "cg":
         run_ours(args)
     else:
-        {"propagator": run_propagator, "uneven": run_uneven, "ptc": run_ptc, "contract": run_contract}[
-            args.workload](args)
+        {"propagator": run_propagator, "uneven": run_uneven, "ptc": run_ptc, "contract": run_contract,
+         "dslash": run_dslash}[args.workload](args)
 
 
 if __name__ == "__main__":
