@@ -271,6 +271,21 @@ QKX_API int qkx_invert_batch(qkx_batch_job* jobs, int njobs, const qkx_solver_pa
 QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread, int* threads_per_block,
                      double* ms_per_hop);
 
+/* Use this tile (one of the tuner's) for later CG_EO_MIXED solves and
+ * qkx_sloppy_normal calls with this precision and batch size, instead of the
+ * tuned one.  No reference counterpart. */
+QKX_API int qkx_set_tile(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block);
+
+/* out_r = Vector::tm_xxDagTm_xx(.., EE) in_r (lib/lattice_util.cpp:2024) for a
+ * batch, computed the way one inner iteration of CG_EO_MIXED computes A p: the
+ * even sites of in_r rounded to the sloppy precision, then the four sloppy hops
+ * with the given tile (rhs_per_thread x threads_per_block, one of the tuner's;
+ * 0, 0 = the tuned tile).  Odd sites of out_r are zero.  Host buffers in
+ * Vector::M layout.  A hook for checking every tile against the FP64 operator;
+ * no reference counterpart. */
+QKX_API int qkx_sloppy_normal(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
+                              const double* const* in_host, double* const* out_host);
+
 /* ---------------------------------------------------------------- gauge-side stencils
  * The smearing links are a second FP64 gauge field held by the context, used
  * only by the Gaussian smearing: they are set by qkx_ape_smear or

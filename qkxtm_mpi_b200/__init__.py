@@ -68,6 +68,7 @@ SYMBOLS = [
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
     "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
+    "qkx_set_tile", "qkx_sloppy_normal",
     "qkx_plaquette", "qkx_plaquette_loaded", "qkx_project_su3", "qkx_ape_smear", "qkx_load_smearing_gauge",
     "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
@@ -196,6 +197,8 @@ def lib() -> C.CDLL:
         L.qkx_kernel_launches.argtypes = [_vp]
         L.qkx_kernel_launches.restype = C.c_longlong
         L.qkx_tune.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
+        L.qkx_set_tile.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.qkx_sloppy_normal.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), C.POINTER(_vp)]
         L.qkx_plaquette.argtypes = [_vp, _vp, _dp]
         L.qkx_plaquette_loaded.argtypes = [_vp, C.c_int, _dp]
         L.qkx_project_su3.argtypes = [_vp, _vp]
@@ -591,6 +594,23 @@ class Lattice:
         nr, nt, ms = C.c_int(), C.c_int(), C.c_double()
         check(lib().qkx_tune(self.ctx, precision, nrhs, C.byref(nr), C.byref(nt), C.byref(ms)))
         return nr.value, nt.value, ms.value
+
+    def set_tile(self, precision: int, nrhs: int, tile) -> None:
+        """Use this hop tile (rhs_per_thread, threads_per_block) for later mixed solves of this
+        precision and batch size instead of the tuned one."""
+        check(lib().qkx_set_tile(self.ctx, precision, nrhs, int(tile[0]), int(tile[1])))
+
+    def sloppy_normal(self, psis: Sequence[np.ndarray], precision: int = PREC_HALF, tile=(0, 0)) -> list:
+        """tm_xxDagTm_xx(EE) of every field as the mixed solver's inner iteration computes it: the
+        even sites rounded to the sloppy precision and the four sloppy hops with the given tile
+        (rhs_per_thread, threads_per_block); (0, 0) = the tuned tile.  Odd sites of the results are zero."""
+        psis = [_host(p) for p in psis]
+        outs = [np.zeros_like(p) for p in psis]
+        n = len(psis)
+        ip = (_vp * n)(*[p.ctypes.data for p in psis])
+        op = (_vp * n)(*[o.ctypes.data for o in outs])
+        check(lib().qkx_sloppy_normal(self.ctx, precision, n, int(tile[0]), int(tile[1]), ip, op))
+        return outs
 
     def kernel_launches(self) -> int:
         return int(lib().qkx_kernel_launches(self.ctx))

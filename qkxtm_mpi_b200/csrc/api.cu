@@ -976,6 +976,27 @@ int qkx_tune(qkx_ctx* c, int precision, int nrhs, int* rhs_per_thread, int* thre
   return tune(c, precision, nrhs, rhs_per_thread, threads_per_block, ms_per_hop);
 }
 
+int qkx_set_tile(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block) {
+  if (!c) return invalid("ctx is NULL");
+  if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
+  return set_tile(c, precision, nrhs, rhs_per_thread, threads_per_block);
+}
+
+int qkx_sloppy_normal(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
+                      const double* const* in_host, double* const* out_host) {
+  if (!c) return invalid("ctx is NULL");
+  if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
+  if (!in_host || !out_host) return invalid("in_host/out_host is NULL");
+  for (int i = 0; i < nrhs; i++)
+    if (!in_host[i] || !out_host[i]) return invalid("a spinor pointer is NULL");
+  if (!c->have_gauge) {
+    set_error("the operator needs a gauge field");
+    return QKX_ERR_NOGAUGE;
+  }
+  QKX_CUDA(cudaSetDevice(c->device));
+  return sloppy_normal(c, precision, nrhs, rhs_per_thread, threads_per_block, in_host, out_host);
+}
+
 int qkx_profile_reset(qkx_ctx* c) {
   if (!c) return invalid("ctx is NULL");
   QKX_TRY(prof_collect(c));

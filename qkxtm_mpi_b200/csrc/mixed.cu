@@ -34,6 +34,7 @@
 #include "blas.cuh"
 #include "hop.cuh"
 #include "hop_mrhs.cuh"
+#include "hop_pair.cuh"
 #include "qkx_ctx.cuh"
 #include "site_ops.cuh"
 
@@ -243,6 +244,19 @@ __global__ void k_mx_from_f64(SpinorF64 src, SOUT dst, const int* active) {
   Spinor<ROUT> o;
 #pragma unroll
   for (int k = 0; k < 12; k++) o.c[k / 3][k % 3] = {ROUT(v.c[k / 3][k % 3].re), ROUT(v.c[k / 3][k % 3].im)};
+  dst.shift(r).store(0, cb, o);
+}
+
+// dst(rhs r) = src(rhs r) widened to FP64, every RHS of the batch
+template <class SIN, typename RIN>
+__global__ void k_mx_to_f64(SIN src, SpinorF64 dst) {
+  const int r = blockIdx.y;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= dst.Vh) return;
+  Spinor<RIN> v = src.shift(r).load(0, cb);
+  Spinor<double> o;
+#pragma unroll
+  for (int k = 0; k < 12; k++) o.c[k / 3][k % 3] = {double(v.c[k / 3][k % 3].re), double(v.c[k / 3][k % 3].im)};
   dst.shift(r).store(0, cb, o);
 }
 
@@ -458,7 +472,10 @@ static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in
   A.active = c->sc->active;
   const int ngrp = (R_ + NR - 1) / NR;
   if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
-  hop_mrhs_kernel<NT, NR, SP, GA, R, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  if constexpr (std::is_same<SP, SpinorF16>::value && std::is_same<GA, GaugeF16x12>::value && NR % 2 == 0)
+    hop_pair_kernel<NT, NR / 2, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  else
+    hop_mrhs_kernel<NT, NR, SP, GA, R, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
   counted(c);
   QKX_CUDA(cudaGetLastError());
   if (prof_slot >= 0)
@@ -887,6 +904,106 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
 }
 
 // the captured graph holds gauge geometry: drop it when the gauge changes
+// out_r = g5 Mh(-) g5 Mh(+) in_r on the even sites (Vector::tm_xxDagTm_xx(.., EE)),
+// computed as one inner iteration of the mixed solver computes A p: the input
+// rounded to the sloppy precision, then the four sloppy hops with the given tile.
+template <class P>
+static int sloppy_normal_t(qkx_ctx* c, int R_, HopTile tile, const double* const* in_host, double* const* out_host) {
+  using SL = Sloppy<P>;
+  using SP = typename P::SP;
+  using GA = typename P::GA;
+  using R = typename P::R;
+  using FT = FieldTraits<SP>;
+  QKX_TRY(mixed_alloc<P>(c, R_, true));
+  MixedState* m = c->mixed;
+  if (tile.nr == 0) QKX_TRY(tile_for<P>(c, R_, &tile));
+  const int Vh = c->Vh;
+  const size_t n12 = 12 * (size_t)Vh;
+  const double k = c->p.kappa, cc = 2.0 * k * c->p.mu * c->p.twistSign;
+  std::vector<double> cv(R_, cc), sv(R_, 1.0 / (1.0 + cc * cc));
+  CgScalars* sh = c->sc_h;
+  memset(sh, 0, sizeof(CgScalars));
+  for (int i = 0; i < R_; i++) sh->active[i] = 1;
+  QKX_CUDA(cudaMemcpyAsync(m->cvec, cv.data(), sizeof(double) * R_, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemcpyAsync(m->svec, sv.data(), sizeof(double) * R_, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemcpyAsync(c->sc, sh, sizeof(CgScalars), cudaMemcpyHostToDevice, c->st));
+  double2* full = nullptr;
+  QKX_CUDA(cudaMallocAsync(&full, sizeof(double2) * 2 * n12, c->st));
+  int rc = QKX_OK;
+  for (int i = 0; i < R_ && rc == QKX_OK; i++) {
+    rc = upload_spinor(c, in_host[i], full);
+    if (rc == QKX_OK && cudaMemcpyAsync(m->bE + i * n12, full, sizeof(double2) * n12, cudaMemcpyDeviceToDevice,
+                                        c->st) != cudaSuccess)
+      rc = QKX_ERR_CUDA;
+  }
+  const dim3 cg2((Vh + 255) / 256, R_);
+  const double k2 = k * k;
+  const GA U = SL::gauge(c);
+  const Geom g = SL::geom(c);
+  SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh), Ap = FT::acc(m->Ap, 0, Vh);
+  if (rc == QKX_OK) {
+    k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->bE, 0, Vh), p, nullptr);
+    counted(c);
+    rc = hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, p, t, p, 1, 0.0, +1.0, true, nullptr, -1);
+  }
+  if (rc == QKX_OK) rc = hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, y, p, 0, -k2, +1.0, false, nullptr, -1);
+  if (rc == QKX_OK) rc = hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr, -1);
+  if (rc == QKX_OK) rc = hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr, -1);
+  if (rc == QKX_OK) {
+    k_mx_to_f64<SP, R><<<cg2, 256, 0, c->st>>>(Ap, B64(m->z64, 0, Vh));
+    counted(c);
+    if (cudaGetLastError() != cudaSuccess) rc = QKX_ERR_CUDA;
+  }
+  for (int i = 0; i < R_ && rc == QKX_OK; i++) {
+    if (cudaMemcpyAsync(full, m->z64 + i * n12, sizeof(double2) * n12, cudaMemcpyDeviceToDevice, c->st) !=
+            cudaSuccess ||
+        cudaMemsetAsync(full + n12, 0, sizeof(double2) * n12, c->st) != cudaSuccess)
+      rc = QKX_ERR_CUDA;
+    if (rc == QKX_OK) rc = download_spinor(c, full, out_host[i]);
+    if (rc == QKX_OK && cudaStreamSynchronize(c->st) != cudaSuccess) rc = QKX_ERR_CUDA;
+  }
+  cudaFreeAsync(full, c->st);
+  if (rc == QKX_ERR_CUDA) set_error("sloppy normal operator: %s", cudaGetErrorString(cudaGetLastError()));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+  return rc;
+}
+
+static bool known_tile(int nr, int nt) {
+  for (const HopTile& t : kTiles)
+    if (t.nr == nr && t.nt == nt) return true;
+  set_error("invalid argument: tile (%d, %d) is not one of the tuner's tiles", nr, nt);
+  return false;
+}
+
+int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt) {
+  if (precision != QKX_PREC_HALF && precision != QKX_PREC_SINGLE && precision != QKX_PREC_DOUBLE) {
+    set_error("invalid argument: precision");
+    return QKX_ERR_INVALID;
+  }
+  if (!known_tile(nr, nt)) return QKX_ERR_INVALID;
+  c->tuned[precision * 1000 + nrhs] = {nr, nt};
+  return QKX_OK;
+}
+
+int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, const double* const* in_host,
+                  double* const* out_host) {
+  HopTile tile;
+  if (nr != 0 || nt != 0) {
+    if (!known_tile(nr, nt)) return QKX_ERR_INVALID;
+    tile.nr = nr;
+    tile.nt = nt;
+  }
+  if (precision != QKX_PREC_DOUBLE && !c->compressible) {
+    set_error("the sloppy operator needs SU(3) links (12-real reconstruction)");
+    return QKX_ERR_UNSUPPORTED;
+  }
+  if (precision == QKX_PREC_HALF) return sloppy_normal_t<PHalf>(c, nrhs, tile, in_host, out_host);
+  if (precision == QKX_PREC_SINGLE) return sloppy_normal_t<PSingle>(c, nrhs, tile, in_host, out_host);
+  if (precision == QKX_PREC_DOUBLE) return sloppy_normal_t<PDouble>(c, nrhs, tile, in_host, out_host);
+  set_error("invalid argument: precision");
+  return QKX_ERR_INVALID;
+}
+
 void mixed_invalidate(qkx_ctx* c) {
   MixedState* m = c->mixed;
   if (m && m->graph) {

@@ -133,6 +133,9 @@ int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
                    qkx_solve_info* info);
 void mixed_invalidate(qkx_ctx* c);
 int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
+int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt);
+int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, const double* const* in_host,
+                  double* const* out_host);
 
 // lazy buffers and context-level helpers (api.cu)
 int ensure_stage(qkx_ctx* c);

@@ -153,3 +153,59 @@ def test_autotuner_picks_a_tile_and_results_are_unchanged(qkx, oracle, setup8):
     xa, ia = lat.invert(bs, precision=qkx.PREC_SINGLE, tol=TOL)
     for b, x in zip(bs, xa):
         assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
+
+
+TILES = [(nr, nt) for nr in (1, 2, 3, 4) for nt in (64, 128, 256)]
+
+
+@pytest.mark.parametrize("prec,tol", [("half", 1e-2), ("single", 1e-5), ("double", 1e-12)])
+def test_sloppy_normal_operator_every_tile(qkx, oracle, setup8, prec, tol):
+    """Each hop tile computes tm_xxDagTm_xx(EE) (the mixed solver's A p): the scalar
+    kernels for any number of right-hand sides per thread and, in half precision, the
+    packed-pair kernels for an even number.  Five right-hand sides, so the last group
+    has lanes outside the batch.  Tolerances: input and three intermediate fields
+    rounded to FP16 (2^-11 of the site maximum) or FP32; FP64 arithmetic throughout."""
+    L, U, lat = setup8
+    p = {"half": qkx.PREC_HALF, "single": qkx.PREC_SINGLE, "double": qkx.PREC_DOUBLE}[prec]
+    bs = [oracle.spinor_gaussian(L, 80 + i) for i in range(5)]
+    exp = [oracle.apply("tm_xx_dagtm_xx_ee", L, U, b, 0.1615, 0.004) for b in bs]
+    first = None
+    for tile in TILES:
+        got = lat.sloppy_normal(bs, p, tile)
+        for g, e in zip(got, exp):
+            assert rel(g, e) < tol, (prec, tile, rel(g, e))
+        if first is None:
+            first = got
+        else:  # the tiles differ only in the order of the FP rounding
+            for g, f in zip(got, first):
+                assert rel(g, f) < tol
+    with pytest.raises(qkx.QkxError) as e:
+        lat.sloppy_normal(bs, p, (5, 64))
+    assert e.value.code == qkx.ERR_INVALID
+
+
+@pytest.mark.parametrize("tile", [(1, 128), (2, 64), (2, 256), (3, 64), (4, 128)])
+def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
+    """Solves with the tile forced: three masses in a batch of five, so right-hand sides
+    leave the batch at different iterations (the per-RHS active mask) and the last
+    group of the tile is partly outside the batch."""
+    import ctypes as C
+    L, U, lat = setup8
+    mus = [0.0015, 0.01, 0.004, 0.02, 0.0015]
+    bs = [oracle.spinor_gaussian(L, 90 + i) for i in range(5)]
+    xs = [np.empty_like(b) for b in bs]
+    n = len(bs)
+    lat.set_tile(qkx.PREC_HALF, n, tile)
+    arr = (C.c_double * n)(*mus)
+    sp = qkx.SolverParams(qkx.SOLVER_CG_EO_MIXED, qkx.PREC_HALF, TOL, 10000, 0.0, 1,
+                          C.cast(arr, C.POINTER(C.c_double)))
+    info = qkx.SolveInfo()
+    bp = (C.c_void_p * n)(*[b.ctypes.data for b in bs])
+    xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+    qkx.check(qkx.lib().qkx_invert(lat.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
+    assert info.converged == 1
+    for mu, b, x in zip(mus, bs, xs):
+        assert true_res(oracle, L, U, x, b, 0.1615, mu) <= TOL
+    with pytest.raises(qkx.QkxError) as e:
+        lat.set_tile(qkx.PREC_HALF, n, (2, 100))
+    assert e.value.code == qkx.ERR_INVALID
