@@ -171,7 +171,8 @@ def run_ours(args):
     barrier = D.barrier
 
     # autotune the inner hop for this lattice and batch (cached in the context)
-    tile = lat.tune(prec, NSRC)
+    lat.tune(prec, NSRC)
+    tile = min(lat.tune_table(prec, NSRC), key=lambda e: e["ms_per_hop"])["tile"]
     for _ in range(args.warmup):
         solve()
     lat.sync()
@@ -286,8 +287,8 @@ def run_ours(args):
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {
-            "kernel": (f"hop_mrhs_kernel<{args.precision} spinors, 12-real links, {NSRC}-RHS batch, "
-                       f"{tile[0]} RHS/thread, {tile[1]} threads/block>"),
+            "kernel": (f"{hop_kernel_name(args.precision, tile)}<{args.precision} spinors, 12-real links, "
+                       f"{NSRC}-RHS batch, {tile[0]} RHS/thread, {tile[1]} threads/block, kind {tile[2]}>"),
             "bound": "hbm",
             "achieved": achieved,
             "peak": peak,
@@ -378,6 +379,21 @@ def _roofline(kernel, launches, ms, nbytes, traffic=None):
             "algorithmic_bytes_per_launch": per}
 
 
+def hop_kernel_name(precision, tile):
+    """The sloppy hop kernel a tile (rhs_per_thread, threads_per_block, kind) launches."""
+    if 1 <= tile[2] <= 3:
+        return "hop_pair_pf_kernel"
+    if tile[2] == 10:
+        return "hop_pair_hm_kernel"
+    if tile[2] >= 8:
+        return "hop_pair_hp_kernel"
+    if tile[2] >= 5:
+        return "hop_pair_as_kernel"
+    if precision in ("half", "fp16") and tile[0] % 2 == 0:
+        return "hop_pair_kernel"
+    return "hop_mrhs_kernel"
+
+
 def run_dslash(args):
     import numpy as np
     import torch
@@ -391,11 +407,15 @@ def run_dslash(args):
     with ClockSampler(0) as clk:
         for name, prec, S, G in (("fp16", Q.PREC_HALF, 52.0, 24.0), ("fp32", Q.PREC_SINGLE, 96.0, 48.0)):
             nr, nt, ms = lat.tune(prec, NSRC)  # CUDA events around 3 pairs of Schur hops per tile, best tile
+            table = lat.tune_table(prec, NSRC)
+            best = min(table, key=lambda e: e["ms_per_hop"])["tile"]
             # one output parity: input and output spinors, links shared by the batch, the
             # xpay operand on every second hop of the pair
             nbytes = Vh * NSRC * (2.5 * S + 8.0 * G / NSRC)
-            hops[name] = {"tile": [nr, nt], "ms_per_hop": ms, "gbs": nbytes / (ms * 1e-3) / 1e9,
-                          "algorithmic_bytes_per_hop": nbytes}
+            hops[name] = {"tile": best, "ms_per_hop": ms, "gbs": nbytes / (ms * 1e-3) / 1e9,
+                          "algorithmic_bytes_per_hop": nbytes,
+                          "tiles_ms_per_hop": {",".join(map(str, e["tile"])): round(e["ms_per_hop"], 4)
+                                               for e in table}}
         a = lat.field(np.random.default_rng(1).standard_normal((lat.V, 4, 3, 2)))
         b = lat.field()
         for _ in range(args.warmup):
@@ -416,10 +436,12 @@ def run_dslash(args):
     lat_s = "x".join(map(str, Lw))
     _common(args, f"Dslash HBM GB/s: even-odd hop, {NSRC} RHS, FP16 spinors and 12-real links, {lat_s}",
             hops["fp16"]["gbs"], "GB/s", True,
-            f"hop_mrhs_kernel on one parity of {lat_s} for a batch of {NSRC} right-hand sides (autotuned tile), "
+            f"{hop_kernel_name('half', hops['fp16']['tile'])} on one parity of {lat_s} for a batch of {NSRC} "
+            f"right-hand sides (autotuned tile {hops['fp16']['tile']}), "
             f"kappa={KAPPA}, mu={MU}; FP64 full-lattice M beside it",
-            {"dtype": "f16 storage / f32 arithmetic", "fp32": hops["fp32"], "fp64_tm": fp64,
-             "roofline": {"kernel": "hop_mrhs_kernel<fp16>", "bound": "hbm", "achieved": hops["fp16"]["gbs"],
+            {"dtype": "f16 storage / f32 arithmetic", "fp16": hops["fp16"], "fp32": hops["fp32"], "fp64_tm": fp64,
+             "roofline": {"kernel": hop_kernel_name("half", hops["fp16"]["tile"]) + "<fp16>", "bound": "hbm",
+                          "achieved": hops["fp16"]["gbs"],
                           "peak": peak, "peak_source": src, "unit": "GB/s", "frac": hops["fp16"]["gbs"] / peak,
                           "traffic": None, "algorithmic_bytes_per_launch": hops["fp16"]["algorithmic_bytes_per_hop"],
                           "avg_launch_ms": hops["fp16"]["ms_per_hop"]},

@@ -271,20 +271,37 @@ QKX_API int qkx_invert_batch(qkx_batch_job* jobs, int njobs, const qkx_solver_pa
 QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread, int* threads_per_block,
                      double* ms_per_hop);
 
-/* Use this tile (one of the tuner's) for later CG_EO_MIXED solves and
+/* A tile of the sloppy hop is (rhs_per_thread, threads_per_block, kind).
+ * kind 0 is the plain kernel for any precision; kinds 1-7 are FP16-only
+ * variants for two right-hand sides a thread: loads of the next neighbour term
+ * held in registers (1-3: no / a 128 / a ~100 registers-a-thread launch
+ * bound), the plain pair kernel with a 128-register bound (4), and loads staged
+ * in shared memory by cp.async one (5, 7) or two (6) terms ahead with a 128
+ * (5, 6) or ~100 (7) register bound, and as 5 with the spin projection done in
+ * FP16 before widening to FP32 (8) and also 18-real FP32 links (9), or also
+ * the link multiply in FP16 on 18-real FP16 links (10; rounds the products to
+ * FP16, so qkx_tune never picks it: only qkx_set_tile selects it).
+ *
+ * Use this tile (one of the tuner's) for later CG_EO_MIXED solves and
  * qkx_sloppy_normal calls with this precision and batch size, instead of the
  * tuned one.  No reference counterpart. */
-QKX_API int qkx_set_tile(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block);
+QKX_API int qkx_set_tile(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
+                         int kind);
+
+/* The per-tile timings of the last tuning of (precision, nrhs): *count tiles,
+ * the first min(*count, max) written to the arrays (any may be NULL).  0 tiles
+ * if that key was never tuned.  No reference counterpart. */
+QKX_API int qkx_tune_table(qkx_ctx* ctx, int precision, int nrhs, int max, int* count, int* rhs_per_thread,
+                           int* threads_per_block, int* kind, double* ms_per_hop);
 
 /* out_r = Vector::tm_xxDagTm_xx(.., EE) in_r (lib/lattice_util.cpp:2024) for a
  * batch, computed the way one inner iteration of CG_EO_MIXED computes A p: the
  * even sites of in_r rounded to the sloppy precision, then the four sloppy hops
- * with the given tile (rhs_per_thread x threads_per_block, one of the tuner's;
- * 0, 0 = the tuned tile).  Odd sites of out_r are zero.  Host buffers in
+ * with the given tile (one of the tuner's; 0, 0, 0 = the tuned tile).  Odd sites of out_r are zero.  Host buffers in
  * Vector::M layout.  A hook for checking every tile against the FP64 operator;
  * no reference counterpart. */
 QKX_API int qkx_sloppy_normal(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
-                              const double* const* in_host, double* const* out_host);
+                              int kind, const double* const* in_host, double* const* out_host);
 
 /* ---------------------------------------------------------------- gauge-side stencils
  * The smearing links are a second FP64 gauge field held by the context, used

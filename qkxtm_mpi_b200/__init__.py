@@ -68,7 +68,7 @@ SYMBOLS = [
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
     "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
-    "qkx_set_tile", "qkx_sloppy_normal",
+    "qkx_set_tile", "qkx_tune_table", "qkx_sloppy_normal",
     "qkx_plaquette", "qkx_plaquette_loaded", "qkx_project_su3", "qkx_ape_smear", "qkx_load_smearing_gauge",
     "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
@@ -197,8 +197,10 @@ def lib() -> C.CDLL:
         L.qkx_kernel_launches.argtypes = [_vp]
         L.qkx_kernel_launches.restype = C.c_longlong
         L.qkx_tune.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
-        L.qkx_set_tile.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int]
-        L.qkx_sloppy_normal.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp), C.POINTER(_vp)]
+        L.qkx_set_tile.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
+        L.qkx_tune_table.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _vp, _vp, _vp, _vp]
+        L.qkx_sloppy_normal.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp),
+                                        C.POINTER(_vp)]
         L.qkx_plaquette.argtypes = [_vp, _vp, _dp]
         L.qkx_plaquette_loaded.argtypes = [_vp, C.c_int, _dp]
         L.qkx_project_su3.argtypes = [_vp, _vp]
@@ -596,20 +598,34 @@ class Lattice:
         return nr.value, nt.value, ms.value
 
     def set_tile(self, precision: int, nrhs: int, tile) -> None:
-        """Use this hop tile (rhs_per_thread, threads_per_block) for later mixed solves of this
-        precision and batch size instead of the tuned one."""
-        check(lib().qkx_set_tile(self.ctx, precision, nrhs, int(tile[0]), int(tile[1])))
+        """Use this hop tile (rhs_per_thread, threads_per_block[, kind]) for later mixed solves of
+        this precision and batch size instead of the tuned one."""
+        t = tuple(tile) + (0,) * (3 - len(tile))
+        check(lib().qkx_set_tile(self.ctx, precision, nrhs, int(t[0]), int(t[1]), int(t[2])))
 
-    def sloppy_normal(self, psis: Sequence[np.ndarray], precision: int = PREC_HALF, tile=(0, 0)) -> list:
+    def tune_table(self, precision: int = PREC_HALF, nrhs: int = 12) -> list:
+        """Every tile timed by the last tuning of (precision, nrhs): dicts with the tile
+        (rhs_per_thread, threads_per_block, kind) and its ms per hop."""
+        n = C.c_int()
+        check(lib().qkx_tune_table(self.ctx, precision, nrhs, 0, C.byref(n), None, None, None, None))
+        k = n.value
+        nr, nt, kd = (C.c_int * max(k, 1))(), (C.c_int * max(k, 1))(), (C.c_int * max(k, 1))()
+        ms = (C.c_double * max(k, 1))()
+        check(lib().qkx_tune_table(self.ctx, precision, nrhs, k, C.byref(n), nr, nt, kd, ms))
+        return [{"tile": [nr[i], nt[i], kd[i]], "ms_per_hop": ms[i]} for i in range(k)]
+
+    def sloppy_normal(self, psis: Sequence[np.ndarray], precision: int = PREC_HALF, tile=(0, 0, 0)) -> list:
         """tm_xxDagTm_xx(EE) of every field as the mixed solver's inner iteration computes it: the
         even sites rounded to the sloppy precision and the four sloppy hops with the given tile
-        (rhs_per_thread, threads_per_block); (0, 0) = the tuned tile.  Odd sites of the results are zero."""
+        (rhs_per_thread, threads_per_block[, kind]); (0, 0, 0) = the tuned tile.  Odd sites of the
+        results are zero."""
         psis = [_host(p) for p in psis]
         outs = [np.zeros_like(p) for p in psis]
         n = len(psis)
         ip = (_vp * n)(*[p.ctypes.data for p in psis])
         op = (_vp * n)(*[o.ctypes.data for o in outs])
-        check(lib().qkx_sloppy_normal(self.ctx, precision, n, int(tile[0]), int(tile[1]), ip, op))
+        t = tuple(tile) + (0,) * (3 - len(tile))
+        check(lib().qkx_sloppy_normal(self.ctx, precision, n, int(t[0]), int(t[1]), int(t[2]), ip, op))
         return outs
 
     def kernel_launches(self) -> int:

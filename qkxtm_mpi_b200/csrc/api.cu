@@ -378,8 +378,10 @@ int download_spinor(qkx_ctx* c, const double2* dev, double* host) {
 
 // ---------------------------------------------------------------- gauge
 // Check the links the operator uses and, if they are SU(3) up to one global
-// sign on the last time slice's t-links, build the 12-real FP32/FP16 copies
-// with that sign stripped (the kernels then apply it from the coordinate).
+// sign on the last time slice's t-links, build the sloppy copies: 12-real
+// FP32 and FP16 with that sign stripped (the kernels then apply it from the
+// coordinate), and 18-real FP32 and FP16 with the sign kept (for the FP16 hop
+// variants that skip the third-row rebuild).
 int gauge_finish(qkx_ctx* c) {
   const int nl = 8 * c->Vh;
   const int nb = (nl + 255) / 256;
@@ -411,6 +413,19 @@ int gauge_finish(qkx_ctx* c) {
       QKX_CUDA(cudaMalloc(&c->U12hb, sizeof(uint2) * 8 * (size_t)c->Vh));
     }
     k_gauge_compress<<<nb, 256, 0, c->st>>>(c->U18, c->geom, c->raw_sign, nullptr, c->U12f, c->U12ha, c->U12hb);
+    counted(c);
+    if (!c->U18fa) {
+      QKX_CUDA(cudaMalloc(&c->U18fa, sizeof(float4) * 8 * 4 * (size_t)c->Vh));
+      QKX_CUDA(cudaMalloc(&c->U18fb, sizeof(float2) * 8 * (size_t)c->Vh));
+    }
+    k_gauge_f32x18<<<nb, 256, 0, c->st>>>(c->U18, c->Vh, c->U18fa, c->U18fb);
+    counted(c);
+    if (!c->U18ha) {
+      QKX_CUDA(cudaMalloc(&c->U18ha, sizeof(uint4) * 8 * (size_t)c->Vh));
+      QKX_CUDA(cudaMalloc(&c->U18hb, sizeof(uint4) * 8 * (size_t)c->Vh));
+      QKX_CUDA(cudaMalloc(&c->U18hc, sizeof(uint32_t) * 8 * (size_t)c->Vh));
+    }
+    k_gauge_f16x18<<<nb, 256, 0, c->st>>>(c->U18, c->Vh, c->U18ha, c->U18hb, c->U18hc);
     counted(c);
     QKX_CUDA(cudaGetLastError());
   }
@@ -506,6 +521,11 @@ void qkx_destroy(qkx_ctx* c) {
   cudaFree(c->U12f);
   cudaFree(c->U12ha);
   cudaFree(c->U12hb);
+  cudaFree(c->U18fa);
+  cudaFree(c->U18fb);
+  cudaFree(c->U18ha);
+  cudaFree(c->U18hb);
+  cudaFree(c->U18hc);
   cudaFree(c->Usm);
   cudaFree(c->stage);
   for (int i = 0; i < qkx_ctx::NW; i++) cudaFree(c->w[i]);
@@ -976,13 +996,20 @@ int qkx_tune(qkx_ctx* c, int precision, int nrhs, int* rhs_per_thread, int* thre
   return tune(c, precision, nrhs, rhs_per_thread, threads_per_block, ms_per_hop);
 }
 
-int qkx_set_tile(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block) {
+int qkx_set_tile(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block, int kind) {
   if (!c) return invalid("ctx is NULL");
   if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
-  return set_tile(c, precision, nrhs, rhs_per_thread, threads_per_block);
+  return set_tile(c, precision, nrhs, rhs_per_thread, threads_per_block, kind);
 }
 
-int qkx_sloppy_normal(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
+int qkx_tune_table(qkx_ctx* c, int precision, int nrhs, int max, int* count, int* rhs_per_thread,
+                   int* threads_per_block, int* kind, double* ms_per_hop) {
+  if (!c) return invalid("ctx is NULL");
+  if (max < 0) return invalid("max must be >= 0");
+  return tune_table(c, precision, nrhs, max, count, rhs_per_thread, threads_per_block, kind, ms_per_hop);
+}
+
+int qkx_sloppy_normal(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int threads_per_block, int kind,
                       const double* const* in_host, double* const* out_host) {
   if (!c) return invalid("ctx is NULL");
   if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
@@ -994,7 +1021,7 @@ int qkx_sloppy_normal(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, i
     return QKX_ERR_NOGAUGE;
   }
   QKX_CUDA(cudaSetDevice(c->device));
-  return sloppy_normal(c, precision, nrhs, rhs_per_thread, threads_per_block, in_host, out_host);
+  return sloppy_normal(c, precision, nrhs, rhs_per_thread, threads_per_block, kind, in_host, out_host);
 }
 
 int qkx_profile_reset(qkx_ctx* c) {

@@ -171,6 +171,41 @@ static __global__ void k_gauge_compress(const double2* __restrict__ eo18, Geom g
   }
 }
 
+// 18-real FP64 (boundary sign included) -> FP32 18 reals: complex 0..7 as four
+// float4 words [parity*4+mu][4][Vh], complex 8 as a float2 [parity*4+mu][Vh]
+static __global__ void k_gauge_f32x18(const double2* __restrict__ eo18, int Vh, float4* __restrict__ a,
+                                      float2* __restrict__ b) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // link index over [2][4][Vh]
+  if (i >= 8 * Vh) return;
+  const int cb = i % Vh, pm = i / Vh;
+  const double2* src = eo18 + (size_t)pm * 9 * Vh + cb;
+  double2 t[9];
+  for (int k = 0; k < 9; k++) t[k] = src[(size_t)k * Vh];
+  for (int q = 0; q < 4; q++)
+    a[(size_t)(pm * 4 + q) * Vh + cb] =
+        make_float4((float)t[2 * q].x, (float)t[2 * q].y, (float)t[2 * q + 1].x, (float)t[2 * q + 1].y);
+  b[(size_t)pm * Vh + cb] = make_float2((float)t[8].x, (float)t[8].y);
+}
+
+// 18-real FP64 (boundary sign included) -> FP16 18 reals as (re, im) half2 words:
+// complex 0..3 and 4..7 as uint4 [parity*4+mu][Vh], complex 8 as uint32
+static __global__ void k_gauge_f16x18(const double2* __restrict__ eo18, int Vh, uint4* __restrict__ a,
+                                      uint4* __restrict__ b, uint32_t* __restrict__ c) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // link index over [2][4][Vh]
+  if (i >= 8 * Vh) return;
+  const int cb = i % Vh, pm = i / Vh;
+  const double2* src = eo18 + (size_t)pm * 9 * Vh + cb;
+  uint32_t w[9];
+  for (int k = 0; k < 9; k++) {
+    const double2 t = src[(size_t)k * Vh];
+    __half2 h = __floats2half2_rn((float)t.x, (float)t.y);
+    w[k] = *reinterpret_cast<uint32_t*>(&h);
+  }
+  a[(size_t)pm * Vh + cb] = make_uint4(w[0], w[1], w[2], w[3]);
+  b[(size_t)pm * Vh + cb] = make_uint4(w[4], w[5], w[6], w[7]);
+  c[(size_t)pm * Vh + cb] = w[8];
+}
+
 // ---------------------------------------------------------------- generators
 // Counter-based generator shared with the CPU oracle: every (seed, stream,
 // counter) hashes to a uniform in (0,1) with the splitmix64 finaliser, and

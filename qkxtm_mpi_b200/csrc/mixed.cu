@@ -347,7 +347,7 @@ struct MixedState {
   double* part = nullptr;  // [R][max(nblk, MX_GRID)]
   cudaGraphExec_t graph = nullptr;
   int graph_R = 0;
-  int graph_nr = 0, graph_nt = 0;  // hop tile the graph was captured with
+  int graph_nr = 0, graph_nt = 0, graph_kind = 0;  // hop tile the graph was captured with
   long long graph_kernels = 0;    // kernel nodes in the graph
   double graph_kappa = 0;         // kappa^2 is a kernel argument inside the graph
   std::vector<cudaEvent_t> gev;   // event pairs captured around the hop kernels
@@ -443,14 +443,33 @@ static int hop_batch(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, 
 }
 
 // ---------------------------------------------------------------- multi-RHS sloppy hop
-// Tile of the sloppy hop: NR right-hand sides per thread, NT threads per block.
+// Tile of the sloppy hop: NR right-hand sides per thread, NT threads per block,
+// and the kernel kind.  Kind 0: hop_mrhs_kernel, or for FP16 with NR even the
+// packed-pair hop_pair_kernel.  FP16 only, NR = 2 (register bounds are
+// launch-bounds hints, 65536 registers / (bound x NT) blocks an SM):
+//   1  hop_pair_pf_kernel, next term's loads held in registers, no bound
+//   2  the same, 128 registers a thread
+//   3  the same, about 100 registers a thread
+//   4  hop_pair_kernel (one pair), 128 registers a thread
+//   5  hop_pair_as_kernel, cp.async into shared memory, one term ahead, 128 registers
+//   6  the same, two terms ahead
+//   7  the same as 5, about 100 registers a thread
+//   8  hop_pair_hp_kernel: as 5 with the spin projection in FP16 before widening
+//   9  the same with 18-real FP32 links (no link conversion or rebuild)
+//  10  hop_pair_hm_kernel: as 8 with the link multiply in FP16 on 18-real FP16 links.
+//      Its products round to FP16, which costs the solver about one more reliable
+//      update on a 32^3x64 batch, so the tuner does not pick it; qkx_set_tile does.
 struct HopTile {
-  int nr = 0, nt = 0;
+  int nr = 0, nt = 0, kind = 0;
 };
-static const HopTile kTiles[] = {{1, 64}, {1, 128}, {1, 256}, {2, 64}, {2, 128}, {2, 256},
-                                 {3, 64}, {3, 128}, {3, 256}, {4, 64}, {4, 128}, {4, 256}};
+static const HopTile kTiles[] = {{1, 64, 0}, {1, 128, 0}, {1, 256, 0}, {2, 64, 0}, {2, 128, 0}, {2, 256, 0},
+                                 {3, 64, 0}, {3, 128, 0}, {3, 256, 0}, {4, 64, 0}, {4, 128, 0}, {4, 256, 0},
+                                 {2, 64, 1}, {2, 128, 1}, {2, 256, 1}, {2, 64, 2}, {2, 128, 2}, {2, 256, 2},
+                                 {2, 64, 3}, {2, 128, 3}, {2, 64, 4}, {2, 128, 4}, {2, 256, 4}, {2, 64, 5},
+                                 {2, 128, 5}, {2, 64, 6}, {2, 64, 7}, {2, 128, 7}, {2, 64, 8}, {2, 128, 8},
+                                 {2, 64, 9},  {2, 128, 9}, {2, 64, 10}, {2, 128, 10}};
 
-template <int NT, int NR, class SP, class GA, typename R, int EPI>
+template <int NT, int NR, int KIND, class SP, class GA, typename R, int EPI>
 static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x, int out_parity,
                        double a, double csign, bool with_s, double* norm_part, int prof_slot) {
   MixedState* m = c->mixed;
@@ -472,10 +491,39 @@ static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in
   A.active = c->sc->active;
   const int ngrp = (R_ + NR - 1) / NR;
   if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
-  if constexpr (std::is_same<SP, SpinorF16>::value && std::is_same<GA, GaugeF16x12>::value && NR % 2 == 0)
+  constexpr bool f16 = std::is_same<SP, SpinorF16>::value && std::is_same<GA, GaugeF16x12>::value;
+  // blocks an SM must hold: 65536 registers / (128 or about 100 a thread x NT)
+  constexpr int B128 = 512 / NT, B100 = 640 / NT;
+  if constexpr (KIND >= 1 && KIND <= 3) {
+    static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
+    constexpr int MINB = KIND == 1 ? 0 : (KIND == 2 ? B128 : B100);
+    hop_pair_pf_kernel<NT, MINB, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  } else if constexpr (KIND == 4) {
+    static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
+    hop_pair_kernel<NT, 1, 0, false, EPI, B128><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  } else if constexpr (KIND == 8 || KIND == 9) {
+    static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
+    if constexpr (KIND == 8) {
+      const HLinks<false> G{gauge.a, gauge.b};
+      hop_pair_hp_kernel<NT, 2, B128, false, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+    } else {
+      const HLinks<true> G{(const uint4*)c->U18fa, (const uint2*)c->U18fb};
+      hop_pair_hp_kernel<NT, 2, B128, true, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+    }
+  } else if constexpr (KIND == 10) {
+    static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
+    const HLinks18 G{c->U18ha, c->U18hb, c->U18hc};
+    hop_pair_hm_kernel<NT, B128, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+  } else if constexpr (KIND >= 5) {
+    static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
+    constexpr int S = KIND == 6 ? 3 : 2;
+    constexpr int MINB = KIND == 7 ? B100 : B128;
+    hop_pair_as_kernel<NT, S, MINB, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  } else if constexpr (f16 && NR % 2 == 0) {
     hop_pair_kernel<NT, NR / 2, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
-  else
+  } else {
     hop_mrhs_kernel<NT, NR, SP, GA, R, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
+  }
   counted(c);
   QKX_CUDA(cudaGetLastError());
   if (prof_slot >= 0)
@@ -486,16 +534,26 @@ static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in
 template <class SP, class GA, typename R, int EPI>
 static int hop_tile(qkx_ctx* c, HopTile t, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x,
                     int out_parity, double a, double csign, bool with_s, double* norm_part, int prof_slot) {
-#define QKX_TILE(NR_, NT_)                                                                                  \
-  if (t.nr == NR_ && t.nt == NT_)                                                                         \
-    return launch_mrhs<NT_, NR_, SP, GA, R, EPI>(c, R_, gauge, g, in, out, x, out_parity, a, csign, with_s, \
-                                                 norm_part, prof_slot);
-  QKX_TILE(1, 64) QKX_TILE(1, 128) QKX_TILE(1, 256)
-  QKX_TILE(2, 64) QKX_TILE(2, 128) QKX_TILE(2, 256)
-  QKX_TILE(3, 64) QKX_TILE(3, 128) QKX_TILE(3, 256)
-  QKX_TILE(4, 64) QKX_TILE(4, 128) QKX_TILE(4, 256)
+#define QKX_TILE(NR_, NT_, K_)                                                                              \
+  if (t.nr == NR_ && t.nt == NT_ && t.kind == K_)                                                          \
+    return launch_mrhs<NT_, NR_, K_, SP, GA, R, EPI>(c, R_, gauge, g, in, out, x, out_parity, a, csign,     \
+                                                     with_s, norm_part, prof_slot);
+  QKX_TILE(1, 64, 0) QKX_TILE(1, 128, 0) QKX_TILE(1, 256, 0)
+  QKX_TILE(2, 64, 0) QKX_TILE(2, 128, 0) QKX_TILE(2, 256, 0)
+  QKX_TILE(3, 64, 0) QKX_TILE(3, 128, 0) QKX_TILE(3, 256, 0)
+  QKX_TILE(4, 64, 0) QKX_TILE(4, 128, 0) QKX_TILE(4, 256, 0)
+  if constexpr (std::is_same<SP, SpinorF16>::value && std::is_same<GA, GaugeF16x12>::value) {
+    QKX_TILE(2, 64, 1) QKX_TILE(2, 128, 1) QKX_TILE(2, 256, 1)
+    QKX_TILE(2, 64, 2) QKX_TILE(2, 128, 2) QKX_TILE(2, 256, 2)
+    QKX_TILE(2, 64, 3) QKX_TILE(2, 128, 3)
+    QKX_TILE(2, 64, 4) QKX_TILE(2, 128, 4) QKX_TILE(2, 256, 4)
+    QKX_TILE(2, 64, 5) QKX_TILE(2, 128, 5) QKX_TILE(2, 64, 6)
+    QKX_TILE(2, 64, 7) QKX_TILE(2, 128, 7)
+    QKX_TILE(2, 64, 8) QKX_TILE(2, 128, 8) QKX_TILE(2, 64, 9) QKX_TILE(2, 128, 9)
+    QKX_TILE(2, 64, 10) QKX_TILE(2, 128, 10)
+  }
 #undef QKX_TILE
-  set_error("invalid hop tile (%d, %d)", t.nr, t.nt);
+  set_error("invalid hop tile (%d, %d, kind %d) for this precision", t.nr, t.nt, t.kind);
   return QKX_ERR_INVALID;
 }
 
@@ -591,8 +649,11 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
   *best_ms = 1e30;
   const double k2 = c->p.kappa * c->p.kappa;
   int rc = QKX_OK;
+  std::vector<std::array<double, 4>> log;
   for (const HopTile& tile : kTiles) {
     if (tile.nr > 1 && tile.nr > R_) continue;
+    if (tile.kind != 0 && P::id != QKX_PREC_HALF) continue;
+    if (tile.kind == 10) continue;  // changes the rounding of the operator, chosen explicitly only
     for (int rep = 0; rep < 4 && rc == QKX_OK; rep++) {
       if (rep == 1) rc = cudaEventRecord(e0, c->st) == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
       if (rc == QKX_OK)
@@ -608,6 +669,7 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
     const double per_hop = ms / 6.0;
+    log.push_back({double(tile.nr), double(tile.nt), double(tile.kind), per_hop});
     if (per_hop < *best_ms) {
       *best_ms = per_hop;
       *best = tile;
@@ -615,7 +677,10 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
-  if (rc == QKX_OK) c->tuned[P::id * 1000 + R_] = {best->nr, best->nt};
+  if (rc == QKX_OK) {
+    c->tuned[P::id * 1000 + R_] = {best->nr, best->nt, best->kind};
+    c->tune_log[P::id * 1000 + R_] = log;
+  }
   return rc;
 }
 
@@ -623,8 +688,9 @@ template <class P>
 static int tile_for(qkx_ctx* c, int R_, HopTile* tile) {
   auto it = c->tuned.find(P::id * 1000 + R_);
   if (it != c->tuned.end()) {
-    tile->nr = it->second.first;
-    tile->nt = it->second.second;
+    tile->nr = it->second.nr;
+    tile->nt = it->second.nt;
+    tile->kind = it->second.kind;
     return QKX_OK;
   }
   double ms;
@@ -746,7 +812,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   }
   const bool graphs = sp->use_graphs != 0;
   if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || m->graph_nr != tile.nr ||
-                   m->graph_nt != tile.nt || !graphs || prof)) {
+                   m->graph_nt != tile.nt || m->graph_kind != tile.kind || !graphs || prof)) {
     cudaGraphExecDestroy(m->graph);
     m->graph = nullptr;
   }
@@ -770,6 +836,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     m->graph_kappa = c->p.kappa;
     m->graph_nr = tile.nr;
     m->graph_nt = tile.nt;
+    m->graph_kind = tile.kind;
   }
 
   const int maxIter = sp->maxIter;
@@ -968,30 +1035,46 @@ static int sloppy_normal_t(qkx_ctx* c, int R_, HopTile tile, const double* const
   return rc;
 }
 
-static bool known_tile(int nr, int nt) {
+static bool known_tile(int precision, int nr, int nt, int kind) {
   for (const HopTile& t : kTiles)
-    if (t.nr == nr && t.nt == nt) return true;
-  set_error("invalid argument: tile (%d, %d) is not one of the tuner's tiles", nr, nt);
+    if (t.nr == nr && t.nt == nt && t.kind == kind && (kind == 0 || precision == QKX_PREC_HALF)) return true;
+  set_error("invalid argument: tile (%d, %d, kind %d) is not one of the tuner's tiles for this precision", nr, nt,
+            kind);
   return false;
 }
 
-int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt) {
+int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind) {
   if (precision != QKX_PREC_HALF && precision != QKX_PREC_SINGLE && precision != QKX_PREC_DOUBLE) {
     set_error("invalid argument: precision");
     return QKX_ERR_INVALID;
   }
-  if (!known_tile(nr, nt)) return QKX_ERR_INVALID;
-  c->tuned[precision * 1000 + nrhs] = {nr, nt};
+  if (!known_tile(precision, nr, nt, kind)) return QKX_ERR_INVALID;
+  c->tuned[precision * 1000 + nrhs] = {nr, nt, kind};
   return QKX_OK;
 }
 
-int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, const double* const* in_host,
+int tune_table(qkx_ctx* c, int precision, int nrhs, int max, int* count, int* nr, int* nt, int* kind, double* ms) {
+  auto it = c->tune_log.find(precision * 1000 + nrhs);
+  const int n = it == c->tune_log.end() ? 0 : (int)it->second.size();
+  if (count) *count = n;
+  for (int i = 0; i < n && i < max; i++) {
+    const auto& e = it->second[i];
+    if (nr) nr[i] = (int)e[0];
+    if (nt) nt[i] = (int)e[1];
+    if (kind) kind[i] = (int)e[2];
+    if (ms) ms[i] = e[3];
+  }
+  return QKX_OK;
+}
+
+int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind, const double* const* in_host,
                   double* const* out_host) {
   HopTile tile;
-  if (nr != 0 || nt != 0) {
-    if (!known_tile(nr, nt)) return QKX_ERR_INVALID;
+  if (nr != 0 || nt != 0 || kind != 0) {
+    if (!known_tile(precision, nr, nt, kind)) return QKX_ERR_INVALID;
     tile.nr = nr;
     tile.nt = nt;
+    tile.kind = kind;
   }
   if (precision != QKX_PREC_DOUBLE && !c->compressible) {
     set_error("the sloppy operator needs SU(3) links (12-real reconstruction)");

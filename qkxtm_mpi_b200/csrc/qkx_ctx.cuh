@@ -3,6 +3,7 @@
 #include <stdarg.h>
 #include <stdio.h>
 
+#include <array>
 #include <map>
 #include <string>
 #include <utility>
@@ -32,6 +33,10 @@ struct MixedState;
     if (rc_ != QKX_OK) return rc_; \
   } while (0)
 
+struct qkx_tile_rec {
+  int nr = 0, nt = 0, kind = 0;
+};
+
 struct qkx_ctx {
   qkx_params p;
   int device = 0;
@@ -48,6 +53,11 @@ struct qkx_ctx {
   float4* U12f = nullptr;     // [2][4][3][Vh] FP32 12-real, SU(3)
   uint4* U12ha = nullptr;     // [2][4][Vh]  FP16 12-real complex 0..3
   uint2* U12hb = nullptr;     // [2][4][Vh]  FP16 12-real complex 4..5
+  float4* U18fa = nullptr;    // [2][4][4][Vh] FP32 18-real complex 0..7 (boundary sign included)
+  float2* U18fb = nullptr;    // [2][4][Vh]  FP32 18-real complex 8
+  uint4* U18ha = nullptr;     // [2][4][Vh]  FP16 18-real complex 0..3 (boundary sign included)
+  uint4* U18hb = nullptr;     // [2][4][Vh]  FP16 18-real complex 4..7
+  uint32_t* U18hc = nullptr;  // [2][4][Vh]  FP16 18-real complex 8
   double2* Usm = nullptr;     // [2][4][9][Vh] FP64 links of the Gaussian smearing (APE-smeared)
   int have_smear = 0;
   double2* stage = nullptr;   // one host-layout spinor (V*12 double2)
@@ -72,7 +82,10 @@ struct qkx_ctx {
   long long kernels = 0;
   int capturing = 0;          // set while a CUDA graph is being captured
   long long captured = 0;     // kernels recorded into the graph being captured
-  std::map<int, std::pair<int, int>> tuned;  // (precision*1000 + nrhs) -> (RHS per thread, threads per block)
+  // tuned tiles: (precision*1000 + nrhs) -> (RHS per thread, threads per block, kernel kind)
+  std::map<int, qkx_tile_rec> tuned;
+  // every tile timed by the last tuning of a key: (nr, nt, kind, ms per hop)
+  std::map<int, std::vector<std::array<double, 4>>> tune_log;
 };
 
 namespace qkx {
@@ -133,8 +146,9 @@ int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
                    qkx_solve_info* info);
 void mixed_invalidate(qkx_ctx* c);
 int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms);
-int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt);
-int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, const double* const* in_host,
+int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind);
+int tune_table(qkx_ctx* c, int precision, int nrhs, int max, int* count, int* nr, int* nt, int* kind, double* ms);
+int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind, const double* const* in_host,
                   double* const* out_host);
 
 // lazy buffers and context-level helpers (api.cu)

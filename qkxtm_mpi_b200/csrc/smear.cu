@@ -155,7 +155,7 @@ int gauss_tile(qkx_ctx* c, int nrhs, const FieldPtrs& in, const FieldPtrs& scrat
   const int key = 900000 + nrhs;
   auto it = c->tuned.find(key);
   if (it != c->tuned.end()) {
-    *out = {it->second.first, it->second.second};
+    *out = {it->second.nr, it->second.nt};
     return QKX_OK;
   }
   cudaEvent_t a, b;
@@ -186,7 +186,7 @@ int gauss_tile(qkx_ctx* c, int nrhs, const FieldPtrs& in, const FieldPtrs& scrat
   cudaEventDestroy(b);
   if (rc == QKX_ERR_CUDA) set_error("smearing tile timing: %s", cudaGetErrorString(cudaGetLastError()));
   if (rc != QKX_OK) return rc;
-  c->tuned[key] = {best.nr, best.nt};
+  c->tuned[key] = {best.nr, best.nt, 0};
   *out = best;
   return QKX_OK;
 }

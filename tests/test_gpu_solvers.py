@@ -155,7 +155,12 @@ def test_autotuner_picks_a_tile_and_results_are_unchanged(qkx, oracle, setup8):
         assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
 
 
-TILES = [(nr, nt) for nr in (1, 2, 3, 4) for nt in (64, 128, 256)]
+TILES = [(nr, nt, 0) for nr in (1, 2, 3, 4) for nt in (64, 128, 256)]
+# FP16 only: two right-hand sides a thread; loads pipelined through registers or shared
+# memory, with several register bounds
+TILES_F16 = ([(2, nt, k) for k in (1, 2, 4) for nt in (64, 128, 256)] + [(2, 64, 3), (2, 128, 3)] +
+             [(2, 64, 5), (2, 128, 5), (2, 64, 6), (2, 64, 7), (2, 128, 7), (2, 64, 8), (2, 128, 8),
+              (2, 64, 9), (2, 128, 9), (2, 64, 10), (2, 128, 10)])
 
 
 @pytest.mark.parametrize("prec,tol", [("half", 1e-2), ("single", 1e-5), ("double", 1e-12)])
@@ -170,7 +175,7 @@ def test_sloppy_normal_operator_every_tile(qkx, oracle, setup8, prec, tol):
     bs = [oracle.spinor_gaussian(L, 80 + i) for i in range(5)]
     exp = [oracle.apply("tm_xx_dagtm_xx_ee", L, U, b, 0.1615, 0.004) for b in bs]
     first = None
-    for tile in TILES:
+    for tile in TILES + (TILES_F16 if prec == "half" else []):
         got = lat.sloppy_normal(bs, p, tile)
         for g, e in zip(got, exp):
             assert rel(g, e) < tol, (prec, tile, rel(g, e))
@@ -179,12 +184,15 @@ def test_sloppy_normal_operator_every_tile(qkx, oracle, setup8, prec, tol):
         else:  # the tiles differ only in the order of the FP rounding
             for g, f in zip(got, first):
                 assert rel(g, f) < tol
-    with pytest.raises(qkx.QkxError) as e:
-        lat.sloppy_normal(bs, p, (5, 64))
-    assert e.value.code == qkx.ERR_INVALID
+    for bad in [(5, 64, 0)] + ([] if prec == "half" else [(2, 128, 1)]):
+        with pytest.raises(qkx.QkxError) as e:
+            lat.sloppy_normal(bs, p, bad)
+        assert e.value.code == qkx.ERR_INVALID
 
 
-@pytest.mark.parametrize("tile", [(1, 128), (2, 64), (2, 256), (3, 64), (4, 128)])
+@pytest.mark.parametrize("tile", [(1, 128, 0), (2, 64, 0), (2, 256, 0), (3, 64, 0), (4, 128, 0), (2, 128, 1),
+                                  (2, 256, 2), (2, 64, 3), (2, 128, 4), (2, 128, 5), (2, 64, 6), (2, 64, 7),
+                                  (2, 64, 8), (2, 128, 9), (2, 64, 10)])
 def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
     """Solves with the tile forced: three masses in a batch of five, so right-hand sides
     leave the batch at different iterations (the per-RHS active mask) and the last
@@ -207,5 +215,5 @@ def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
     for mu, b, x in zip(mus, bs, xs):
         assert true_res(oracle, L, U, x, b, 0.1615, mu) <= TOL
     with pytest.raises(qkx.QkxError) as e:
-        lat.set_tile(qkx.PREC_HALF, n, (2, 100))
+        lat.set_tile(qkx.PREC_HALF, n, (2, 100, 0))
     assert e.value.code == qkx.ERR_INVALID
