@@ -170,9 +170,14 @@ def run_ours(args):
 
     barrier = D.barrier
 
-    # autotune the inner hop for this lattice and batch (cached in the context)
-    lat.tune(prec, NSRC)
-    tile = min(lat.tune_table(prec, NSRC), key=lambda e: e["ms_per_hop"])["tile"]
+    # autotune the inner hop for this lattice and batch (cached in the context), or use
+    # the tile given on the command line (so that a profiler run launches the same kernel)
+    if args.tile:
+        tile = list(args.tile) + [0] * (3 - len(args.tile))
+        lat.set_tile(prec, NSRC, tile)
+    else:
+        lat.tune(prec, NSRC)
+        tile = min(lat.tune_table(prec, NSRC), key=lambda e: e["ms_per_hop"])["tile"]
     for _ in range(args.warmup):
         solve()
     lat.sync()
@@ -721,6 +726,8 @@ def main():
     ap.add_argument("--ptc-steps", type=int, default=2000)
     ap.add_argument("--lattice", type=lambda v: tuple(int(x) for x in v.split(",")), default=L,
                     help="X,Y,Z,T for the non-default workloads")
+    ap.add_argument("--tile", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
+                    help="RHS_PER_THREAD,THREADS_PER_BLOCK,KIND of the sloppy hop instead of the autotuner's")
     args = ap.parse_args()
     if args.warmup < 3:
         print("note: --warmup below 3 raised to 3", file=sys.stderr)
