@@ -155,6 +155,7 @@ def run_ours(args):
     lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, twistSign=1, boundaryT=-1, tol=TOL,
                                   maxIter=5000), device=local)
     lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
+    lat.set_fp64_traversal(args.fp64_traversal)
     t_src = D.source_timeslice(rank, L[3])
     srcs = point_sources(np, t_src)
     bd = [lat.field(b) for b in srcs]
@@ -289,6 +290,10 @@ def run_ours(args):
         "iterations": it,
         "reliable_updates": max(i.reliable_updates for i in infos),
         "true_residual_max": max(i.true_residual for i in infos),
+        # device time per solve by phase (medians over the timed solves)
+        "phases_s": {k: round(float(np.median([getattr(i, a) for i in infos])), 5) for k, a in (
+            ("setup", "seconds_setup"), ("reliable_updates", "seconds_reliable"), ("final", "seconds_final"),
+            ("solve", "seconds"))},
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {
@@ -726,6 +731,8 @@ def main():
     ap.add_argument("--ptc-steps", type=int, default=2000)
     ap.add_argument("--lattice", type=lambda v: tuple(int(x) for x in v.split(",")), default=L,
                     help="X,Y,Z,T for the non-default workloads")
+    ap.add_argument("--fp64-traversal", type=int, default=-1,
+                    help="order of the FP64 hop: -1 automatic, 0 cb order, k>0 chunks of k site blocks")
     ap.add_argument("--tile", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
                     help="RHS_PER_THREAD,THREADS_PER_BLOCK,KIND of the sloppy hop instead of the autotuner's")
     args = ap.parse_args()

@@ -199,6 +199,11 @@ typedef struct qkx_solve_info {
   double normal_residual;  /* max over RHS of the final CG residual ||r|| / ||in|| */
   double seconds;          /* device time of the solve (CUDA events) */
   int fallbacks;           /* right-hand sides that QKX_SOLVER_GCR_PTC handed to the plain solver */
+  /* device time of the phases of a CG_EO_MIXED solve (0 for the other methods);
+   * the inner iterations take seconds - setup - reliable - final */
+  double seconds_setup;     /* gathering b, the Schur source b^ and Mh^+ b^ (FP64) */
+  double seconds_reliable;  /* the FP64 reliable updates */
+  double seconds_final;     /* odd sites, the FP64 true residual and the copies out */
 } qkx_solve_info;
 
 /* CG::operator()(out, in, param) (lib/solvers.cpp:16-81), FP64, full lattice:
@@ -287,6 +292,15 @@ QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread,
  * tuned one.  No reference counterpart. */
 QKX_API int qkx_set_tile(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
                          int kind);
+
+/* The order in which the FP64 hopping kernel (every FP64 operator, solver
+ * and reliable update of this context) walks the lattice; the result is the
+ * same in every order.  chunk_blocks = -1 (default): automatic, cb order
+ * unless the right-hand sides of a batch make two t-slices larger than L2,
+ * then chunks of a t-slice walked chunk by chunk; 0: cb order; k > 0: chunks
+ * of k blocks of 64 sites, k dividing the blocks of a t-slice (L0 L1 L2 / 128
+ * of them).  No reference counterpart. */
+QKX_API int qkx_set_fp64_traversal(qkx_ctx* ctx, int chunk_blocks);
 
 /* The per-tile timings of the last tuning of (precision, nrhs): *count tiles,
  * the first min(*count, max) written to the arrays (any may be NULL).  0 tiles

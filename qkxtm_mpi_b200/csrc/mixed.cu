@@ -247,6 +247,16 @@ __global__ void k_mx_from_f64(SpinorF64 src, SOUT dst, const int* active) {
   dst.shift(r).store(0, cb, o);
 }
 
+// dst(rhs r) = src(rhs r) in dst's precision for the active RHS of a batch of single-parity fields
+template <class SIN, class SOUT>
+__global__ void k_mx_convert(SIN src, SOUT dst, const int* active) {
+  const int r = blockIdx.y;
+  if (active && !active[r]) return;
+  int cb = blockIdx.x * blockDim.x + threadIdx.x;
+  if (cb >= src.Vh) return;
+  dst.shift(r).store(0, cb, src.shift(r).load(0, cb));
+}
+
 // dst(rhs r) = src(rhs r) widened to FP64, every RHS of the batch
 template <class SIN, typename RIN>
 __global__ void k_mx_to_f64(SIN src, SpinorF64 dst) {
@@ -351,6 +361,7 @@ struct MixedState {
   long long graph_kernels = 0;    // kernel nodes in the graph
   double graph_kappa = 0;         // kappa^2 is a kernel argument inside the graph
   std::vector<cudaEvent_t> gev;   // event pairs captured around the hop kernels
+  cudaEvent_t ph[3] = {};         // phase marks: set-up done, reliable update start, its end
 };
 
 void mixed_free(qkx_ctx* c) {
@@ -364,6 +375,8 @@ void mixed_free(qkx_ctx* c) {
   cudaFree(m->part);
   if (m->graph) cudaGraphExecDestroy(m->graph);
   for (auto e : m->gev) cudaEventDestroy(e);
+  for (auto e : m->ph)
+    if (e) cudaEventDestroy(e);
   delete m;
   c->mixed = nullptr;
 }
@@ -713,6 +726,32 @@ static int schur64_g5_batch(qkx_ctx* c, int R_, double csign, double2* v, double
                      m->cvec, nullptr, c->sc->active, norm_part, nblk);
 }
 
+// r = g5 Mh(-c) g5 rhat = Mh^+ rhat for the active RHS, in FP32 on the 12-real FP32 links,
+// from the FP64 field z = g5 rhat, into the FP32 field out, with |r|^2 partials per RHS in
+// m->part (*nblk of them).  r is the residual the sloppy CG restarts from, so FP32 is enough:
+// the true residual rhat it is built from is FP64, and the sloppy iterations that continue
+// from r round to FP16 or FP32 themselves.  m->r64 is the scratch (the FP32 copy of z and
+// the odd-parity intermediate, 96 B per site and RHS each).
+static int normal_residual_f32(qkx_ctx* c, int R_, double2* z, SpinorF32 out, int* nblk) {
+  MixedState* m = c->mixed;
+  const int Vh = c->Vh;
+  const double k = c->p.kappa;
+  using F32 = FieldTraits<SpinorF32>;
+  const BField zb{m->r64, nullptr}, tb{(float4*)m->r64 + F32::words * (size_t)Vh * R_, nullptr};
+  const SpinorF32 z32 = F32::acc(zb, 0, Vh), t32 = F32::acc(tb, 1, Vh);
+  const dim3 cg2((Vh + 255) / 256, R_);
+  k_mx_from_f64<SpinorF32, float><<<cg2, 256, 0, c->st>>>(B64(z, 0, Vh), z32, c->sc->active);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  const GaugeF32x12 U{c->U12f, Vh};
+  QKX_TRY((hop_batch<SpinorF32, GaugeF32x12, float, EPI_TWIST_INV>(c, R_, U, c->geom_raw, z32, t32, z32, 1, 0.0,
+                                                                   -1.0, true, nullptr, -1)));
+  QKX_TRY((hop_batch<SpinorF32, GaugeF32x12, float, EPI_XPAY_G5>(c, R_, U, c->geom_raw, t32, out, z32, 0, -k * k,
+                                                                 -1.0, false, m->part, -1)));
+  *nblk = hop_blocks_per_rhs<128>(Vh, 0);
+  return QKX_OK;
+}
+
 template <class P>
 static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
                              double2* const* x, qkx_solve_info* info) {
@@ -745,6 +784,8 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   CgScalars* sh = c->sc_h;
   memset(sh, 0, sizeof(CgScalars));
   for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
+  for (auto& e : m->ph)
+    if (!e) QKX_CUDA(cudaEventCreate(&e));
 
   QKX_CUDA(cudaEventRecord(c->t0, c->st));
   QKX_CUDA(cudaMemcpyAsync(m->cvec, cv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
@@ -776,19 +817,33 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   counted(c);
   k_mx_site<SITE_GAMMA5><<<cg2, 256, 0, c->st>>>(B64(m->z64, 0, Vh), B64(m->g5bh, 0, Vh), 0, nullptr, nullptr);
   counted(c);
-  // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2
-  QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part, &nb64));
+  // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2 (FP32 when the sloppy residual is FP32)
+  constexpr bool r32 = std::is_same<AC, SpinorF32>::value;
+  if constexpr (r32) {
+    QKX_TRY(normal_residual_f32(c, nrhs, m->g5bh, FA::acc(m->rs, 0, Vh), &nb64));
+  } else {
+    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part, &nb64));
+  }
   k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_R2_INIT, c->sc);
   counted(c);
   QKX_CUDA(cudaMemsetAsync(m->x64, 0, hb * nrhs, c->st));
   QKX_CUDA(cudaMemsetAsync(m->xs.d, 0, FA::words * 16 * (size_t)Vh * nrhs, c->st));
-  k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
-  counted(c);
-  k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
-  counted(c);
+  if constexpr (r32) {
+    k_mx_convert<AC, SP><<<cg2, 256, 0, c->st>>>(FA::acc(m->rs, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+    counted(c);
+  } else {
+    k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
+    counted(c);
+    k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+    counted(c);
+  }
   QKX_CUDA(cudaGetLastError());
+  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));
   QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
   QKX_CUDA(cudaStreamSynchronize(c->st));
+  float ms_setup = 0, ms_ru = 0, ms_seg = 0;
+  QKX_CUDA(cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]));
+  bool ru_pending = false;  // a reliable update's end mark not yet read
 
   std::vector<double> bnorm2(nrhs), r2ru(nrhs), ratio(nrhs, 1.0);
   std::vector<int> active(nrhs, 1);
@@ -856,6 +911,11 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     since++;
     QKX_CUDA(cudaMemcpyAsync(sh->r2, c->sc->r2, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, c->st));
     QKX_CUDA(cudaStreamSynchronize(c->st));
+    if (ru_pending) {
+      QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
+      ms_ru += ms_seg;
+      ru_pending = false;
+    }
     if (prof) {
       for (int h = 0; h < 4; h++) {
         float ms = 0;
@@ -879,6 +939,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     if (!ru) continue;
     n_ru++;
     since = 0;
+    QKX_CUDA(cudaEventRecord(m->ph[1], c->st));
     // x64 += x_s ; z = g5 b^ - g5 Mh x64 = g5 rhat ; r = Mh^+ rhat
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
     counted(c);
@@ -887,7 +948,11 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     counted(c);
     k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
     counted(c);
-    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb64));
+    if constexpr (r32) {  // straight into the sloppy residual of the RHS that go on
+      QKX_TRY(normal_residual_f32(c, nrhs, m->z64, FA::acc(m->rs, 0, Vh), &nb64));
+    } else {
+      QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb64));
+    }
     k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
     counted(c);
     QKX_CUDA(cudaGetLastError());
@@ -905,13 +970,24 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
       r2ru[i] = r2;
       sh->r2[i] = r2;
     }
-    // restart the sloppy residual from the FP64 one for the RHS that go on
+    // restart the sloppy residual from the new one for the RHS that go on
     QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
     QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
-    k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
-    counted(c);
+    if constexpr (!r32) {
+      k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
+      counted(c);
+    }
     QKX_CUDA(cudaGetLastError());
+    QKX_CUDA(cudaEventRecord(m->ph[2], c->st));
+    ru_pending = true;
   }
+  if (ru_pending) {
+    QKX_CUDA(cudaEventSynchronize(m->ph[2]));
+    QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
+    ms_ru += ms_seg;
+  }
+  // the final phase starts where the last reliable update or iteration ended
+  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));
   int rc = QKX_OK;
   int nact = 0;
   for (int i = 0; i < nrhs; i++) nact += active[i];
@@ -961,9 +1037,13 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     info->converged = rc == QKX_OK;
     info->true_residual = worst;
     info->normal_residual = 0.0;
-    float ms = 0;
+    float ms = 0, ms_final = 0;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
+    cudaEventElapsedTime(&ms_final, m->ph[0], c->t1);
     info->seconds = ms * 1e-3;
+    info->seconds_setup = ms_setup * 1e-3;
+    info->seconds_reliable = ms_ru * 1e-3;
+    info->seconds_final = ms_final * 1e-3;
   }
   if (rc == QKX_ERR_NOT_CONVERGED)
     set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
