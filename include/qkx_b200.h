@@ -285,7 +285,8 @@ QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread,
  * (5, 6) or ~100 (7) register bound, and as 5 with the spin projection done in
  * FP16 before widening to FP32 (8) and also 18-real FP32 links (9), or also
  * the link multiply in FP16 on 18-real FP16 links (10; rounds the products to
- * FP16, so qkx_tune never picks it: only qkx_set_tile selects it).
+ * FP16, so qkx_tune never picks it: only qkx_set_tile selects it), or as 8
+ * on 18-real FP16 links (11: no third-row rebuild).
  *
  * Use this tile (one of the tuner's) for later CG_EO_MIXED solves and
  * qkx_sloppy_normal calls with this precision and batch size, instead of the

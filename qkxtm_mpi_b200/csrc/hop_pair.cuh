@@ -821,9 +821,10 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1) hop_pair_as_kernel(Ho
 // real/imaginary halves swapped for +-i: one rounding of a sum of two
 // site-normalised values, the size of the storage rounding), and only the six
 // projected complex numbers are widened, so a term converts 12 halves a
-// right-hand side instead of 24.  With L32 the links are the operator's own
-// 18 reals in FP32 (boundary sign included): no conversion, no third-row
-// rebuild.
+// right-hand side instead of 24.  The link format LK: 0 the 12-real FP16 links
+// (row 2 rebuilt, boundary sign from the t coordinate); 1 the operator's own 18
+// reals in FP32 (boundary sign included): no conversion, no third-row rebuild;
+// 2 the 18 reals in FP16 (boundary sign included): nine conversions, no rebuild.
 
 // a + phase<PH>(z) on one (re, im) half2
 template <int PH>
@@ -851,26 +852,32 @@ __device__ __forceinline__ void proj_h(const uint32_t (&w)[12], __half2 (&h)[2][
   }
 }
 
-template <int NT, bool L32>
+template <int NT, int LK>
 struct HSlot {
   uint4 sp[6][NT];
   float nm[2][NT];
-  uint4 la[L32 ? 4 : 1][NT];
-  uint2 lb[NT];  // FP16 complex 4..5, or the FP32 complex 8
+  uint4 la[LK == 1 ? 4 : (LK == 2 ? 2 : 1)][NT];
+  uint2 lb[LK == 2 ? 1 : NT];      // FP16 complex 4..5 (LK 0), or the FP32 complex 8 (LK 1)
+  uint32_t lc[LK == 2 ? NT : 1];   // the FP16 complex 8 (LK 2)
 };
 
-// the links of a variant: FP16 12-real as GaugeF16x12 ([parity*4+mu][Vh] uint4 of
-// complex 0..3 and uint2 of complex 4..5), or FP32 18-real with the boundary sign
-// ([parity*4+mu][4][Vh] float4 of complex 0..7 and [parity*4+mu][Vh] float2 of
-// complex 8, both as raw words)
-template <bool L32>
+// the links of a variant, as raw words:
+//   LK 0: FP16 12-real as GaugeF16x12, [parity*4+mu][Vh] uint4 of complex 0..3 (a)
+//         and uint2 of complex 4..5 (b);
+//   LK 1: FP32 18-real with the boundary sign, [parity*4+mu][4][Vh] float4 of
+//         complex 0..7 (a) and [parity*4+mu][Vh] float2 of complex 8 (b);
+//   LK 2: FP16 18-real with the boundary sign, [parity*4+mu][Vh] uint4 of complex
+//         0..3 (a), uint4 of complex 4..7 (a2) and uint32 of complex 8 (c).
+template <int LK>
 struct HLinks {
   const uint4* a;
   const uint2* b;
+  const uint4* a2 = nullptr;
+  const uint32_t* c = nullptr;
 };
 
-template <int D, int NT, bool L32>
-__device__ __forceinline__ void nb_issue_h(HSlot<NT, L32>& st, int tid, const PairPtrs& P, const HLinks<L32>& G,
+template <int D, int NT, int LK>
+__device__ __forceinline__ void nb_issue_h(HSlot<NT, LK>& st, int tid, const PairPtrs& P, const HLinks<LK>& G,
                                            const Geom& g, int par, int cb, const int x[4], int s, int stride) {
   constexpr int MU = D >> 1;
   const int Lm = g.L[MU];
@@ -891,27 +898,32 @@ __device__ __forceinline__ void nb_issue_h(HSlot<NT, L32>& st, int tid, const Pa
   }
   cpa4(&st.nm[0][tid], P.nj + n);
   cpa4(&st.nm[1][tid], P.nk + n);
-  if constexpr (L32) {
+  if constexpr (LK == 1) {
 #pragma unroll
     for (int q = 0; q < 4; q++) cpa16(&st.la[q][tid], G.a + (size_t)(pm * 4 + q) * g.Vh + li);
+    cpa8(&st.lb[tid], G.b + (size_t)pm * g.Vh + li);
+  } else if constexpr (LK == 2) {
+    cpa16(&st.la[0][tid], G.a + (size_t)pm * g.Vh + li);
+    cpa16(&st.la[1][tid], G.a2 + (size_t)pm * g.Vh + li);
+    cpa4(&st.lc[tid], G.c + (size_t)pm * g.Vh + li);
   } else {
     cpa16(&st.la[0][tid], G.a + (size_t)pm * g.Vh + li);
+    cpa8(&st.lb[tid], G.b + (size_t)pm * g.Vh + li);
   }
-  cpa8(&st.lb[tid], G.b + (size_t)pm * g.Vh + li);
 }
 
-template <int B, bool DAG, int D, int NT, bool L32>
-__device__ __forceinline__ void nb_compute_h(const HSlot<NT, L32>& st, int tid, const Geom& g, const int x[4],
+template <int B, bool DAG, int D, int NT, int LK>
+__device__ __forceinline__ void nb_compute_h(const HSlot<NT, LK>& st, int tid, const Geom& g, const int x[4],
                                              CP (&acc)[4][3]) {
   constexpr int MU = D >> 1;
   constexpr bool BWD = (D & 1) != 0;
   constexpr int SF = DAG ? +1 : -1;
   constexpr int SG = BWD ? -SF : SF;  // projector 1 + SG*g
   bool flip = false;
-  if constexpr (!L32) flip = (MU == 3) && g.bc_sign < 0 && x[3] == (BWD ? 0 : g.L[3] - 1);
+  if constexpr (LK == 0) flip = (MU == 3) && g.bc_sign < 0 && x[3] == (BWD ? 0 : g.L[3] - 1);
   const float sg = (flip ? -1.f : 1.f) * (Proj<B, MU, SG>::diag ? 2.f : 1.f);
   Link<float> u;
-  if constexpr (L32) {
+  if constexpr (LK == 1) {
 #pragma unroll
     for (int q = 0; q < 4; q++) {
       const uint4 w = st.la[q][tid];
@@ -920,6 +932,14 @@ __device__ __forceinline__ void nb_compute_h(const HSlot<NT, L32>& st, int tid, 
     }
     const uint2 w = st.lb[tid];
     u.m[2][2] = {__uint_as_float(w.x), __uint_as_float(w.y)};
+  } else if constexpr (LK == 2) {
+    const uint4 w0 = st.la[0][tid], w1 = st.la[1][tid];
+    const uint32_t ws[9] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, st.lc[tid]};
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+      const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&ws[k]));
+      u.m[k / 3][k % 3] = {f.x, f.y};
+    }
   } else {
     const uint4 w0 = st.la[0][tid];
     const uint2 w1 = st.lb[tid];
@@ -957,11 +977,11 @@ __device__ __forceinline__ void nb_compute_h(const HSlot<NT, L32>& st, int tid, 
   recon_pair<B, MU, SG>(acc, uh, f, fn);
 }
 
-template <int NT, int S, int MINB, bool L32, int B, bool DAG, int EPI>
+template <int NT, int S, int MINB, int LK, int B, bool DAG, int EPI>
 __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
-    hop_pair_hp_kernel(HopArgs<SpinorF16, GaugeF16x12> A, HLinks<L32> G) {
+    hop_pair_hp_kernel(HopArgs<SpinorF16, GaugeF16x12> A, HLinks<LK> G) {
   static_assert(S == 2 || S == 3, "pipeline depth");
-  __shared__ HSlot<NT, L32> st[S];
+  __shared__ HSlot<NT, LK> st[S];
   const int ngrp = (A.nrhs + 1) / 2;
   const int grp = blockIdx.x % ngrp;
   const int blk = blockIdx.x / ngrp;
@@ -996,10 +1016,10 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
     auto issue = [&](auto ic) {
       constexpr int I = decltype(ic)::value;
       if constexpr (I < 8) {
-        nb_issue_h<I, NT, L32>(st[I % S], tid, P, G, g, par, cb, x, s, strd[I >> 1]);
+        nb_issue_h<I, NT, LK>(st[I % S], tid, P, G, g, par, cb, x, s, strd[I >> 1]);
       } else if constexpr (XOP) {
         const SpinorF16 xj = A.x.shift(rj), xk = A.x.shift(rk);
-        HSlot<NT, L32>& t = st[8 % S];
+        HSlot<NT, LK>& t = st[8 % S];
         const uint4* bj = (par ? xj.p1 : xj.p0) + cb;
         const uint4* bk = (par ? xk.p1 : xk.p0) + cb;
 #pragma unroll
@@ -1021,7 +1041,7 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
     auto step = [&](auto dc) {
       constexpr int D = decltype(dc)::value;
       cpa_wait<S - 1>();
-      nb_compute_h<B, DAG, D, NT, L32>(st[D % S], tid, g, x, acc);
+      nb_compute_h<B, DAG, D, NT, LK>(st[D % S], tid, g, x, acc);
       if constexpr (D + S <= 8) issue(std::integral_constant<int, D + S>{});
       else cpa_commit();
     };
@@ -1035,7 +1055,7 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
     step(std::integral_constant<int, 7>{});
     cpa_wait<0>();
     if constexpr (XOP) {
-      const HSlot<NT, L32>& t = st[8 % S];
+      const HSlot<NT, LK>& t = st[8 % S];
       CP xv[4][3];
       const float2 n = make_float2(t.nm[0][tid], t.nm[1][tid]);
 #pragma unroll

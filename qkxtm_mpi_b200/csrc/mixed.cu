@@ -472,6 +472,8 @@ static int hop_batch(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, 
 //  10  hop_pair_hm_kernel: as 8 with the link multiply in FP16 on 18-real FP16 links.
 //      Its products round to FP16, which costs the solver about one more reliable
 //      update on a 32^3x64 batch, so the tuner does not pick it; qkx_set_tile does.
+//  11  as 8 with the 18-real FP16 links (boundary sign included): nine half2
+//      conversions a link and no third-row rebuild, for 12 more bytes a link.
 struct HopTile {
   int nr = 0, nt = 0, kind = 0;
 };
@@ -480,7 +482,8 @@ static const HopTile kTiles[] = {{1, 64, 0}, {1, 128, 0}, {1, 256, 0}, {2, 64, 0
                                  {2, 64, 1}, {2, 128, 1}, {2, 256, 1}, {2, 64, 2}, {2, 128, 2}, {2, 256, 2},
                                  {2, 64, 3}, {2, 128, 3}, {2, 64, 4}, {2, 128, 4}, {2, 256, 4}, {2, 64, 5},
                                  {2, 128, 5}, {2, 64, 6}, {2, 64, 7}, {2, 128, 7}, {2, 64, 8}, {2, 128, 8},
-                                 {2, 64, 9},  {2, 128, 9}, {2, 64, 10}, {2, 128, 10}};
+                                 {2, 64, 9},  {2, 128, 9}, {2, 64, 10}, {2, 128, 10}, {2, 64, 11},
+                                 {2, 128, 11}};
 
 template <int NT, int NR, int KIND, class SP, class GA, typename R, int EPI>
 static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x, int out_parity,
@@ -514,14 +517,17 @@ static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in
   } else if constexpr (KIND == 4) {
     static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
     hop_pair_kernel<NT, 1, 0, false, EPI, B128><<<A.nblk * ngrp, NT, 0, c->st>>>(A);
-  } else if constexpr (KIND == 8 || KIND == 9) {
+  } else if constexpr (KIND == 8 || KIND == 9 || KIND == 11) {
     static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
     if constexpr (KIND == 8) {
-      const HLinks<false> G{gauge.a, gauge.b};
-      hop_pair_hp_kernel<NT, 2, B128, false, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+      const HLinks<0> G{gauge.a, gauge.b};
+      hop_pair_hp_kernel<NT, 2, B128, 0, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+    } else if constexpr (KIND == 9) {
+      const HLinks<1> G{(const uint4*)c->U18fa, (const uint2*)c->U18fb};
+      hop_pair_hp_kernel<NT, 2, B128, 1, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
     } else {
-      const HLinks<true> G{(const uint4*)c->U18fa, (const uint2*)c->U18fb};
-      hop_pair_hp_kernel<NT, 2, B128, true, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
+      const HLinks<2> G{c->U18ha, nullptr, c->U18hb, c->U18hc};
+      hop_pair_hp_kernel<NT, 2, B128, 2, 0, false, EPI><<<A.nblk * ngrp, NT, 0, c->st>>>(A, G);
     }
   } else if constexpr (KIND == 10) {
     static_assert(f16 && NR == 2, "pipelined tiles are FP16 pairs");
@@ -564,6 +570,7 @@ static int hop_tile(qkx_ctx* c, HopTile t, int R_, const GA& gauge, const Geom& 
     QKX_TILE(2, 64, 7) QKX_TILE(2, 128, 7)
     QKX_TILE(2, 64, 8) QKX_TILE(2, 128, 8) QKX_TILE(2, 64, 9) QKX_TILE(2, 128, 9)
     QKX_TILE(2, 64, 10) QKX_TILE(2, 128, 10)
+    QKX_TILE(2, 64, 11) QKX_TILE(2, 128, 11)
   }
 #undef QKX_TILE
   set_error("invalid hop tile (%d, %d, kind %d) for this precision", t.nr, t.nt, t.kind);

@@ -160,7 +160,7 @@ TILES = [(nr, nt, 0) for nr in (1, 2, 3, 4) for nt in (64, 128, 256)]
 # memory, with several register bounds
 TILES_F16 = ([(2, nt, k) for k in (1, 2, 4) for nt in (64, 128, 256)] + [(2, 64, 3), (2, 128, 3)] +
              [(2, 64, 5), (2, 128, 5), (2, 64, 6), (2, 64, 7), (2, 128, 7), (2, 64, 8), (2, 128, 8),
-              (2, 64, 9), (2, 128, 9), (2, 64, 10), (2, 128, 10)])
+              (2, 64, 9), (2, 128, 9), (2, 64, 10), (2, 128, 10), (2, 64, 11), (2, 128, 11)])
 
 
 @pytest.mark.parametrize("prec,tol", [("half", 1e-2), ("single", 1e-5), ("double", 1e-12)])
@@ -192,7 +192,7 @@ def test_sloppy_normal_operator_every_tile(qkx, oracle, setup8, prec, tol):
 
 @pytest.mark.parametrize("tile", [(1, 128, 0), (2, 64, 0), (2, 256, 0), (3, 64, 0), (4, 128, 0), (2, 128, 1),
                                   (2, 256, 2), (2, 64, 3), (2, 128, 4), (2, 128, 5), (2, 64, 6), (2, 64, 7),
-                                  (2, 64, 8), (2, 128, 9), (2, 64, 10)])
+                                  (2, 64, 8), (2, 128, 9), (2, 64, 10), (2, 128, 11)])
 def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
     """Solves with the tile forced: three masses in a batch of five, so right-hand sides
     leave the batch at different iterations (the per-RHS active mask) and the last
