@@ -155,7 +155,6 @@ def run_ours(args):
     lat = Q.Lattice(Q.LatticeInfo(L=L, kappa=KAPPA, mu=MU, twistSign=1, boundaryT=-1, tol=TOL,
                                   maxIter=5000), device=local)
     lat.generate_gauge(EPS, SEED, Q.LINKS_APPLY_BC)
-    lat.set_fp64_traversal(args.fp64_traversal)
     t_src = D.source_timeslice(rank, L[3])
     srcs = point_sources(np, t_src)
     bd = [lat.field(b) for b in srcs]
@@ -261,7 +260,7 @@ def run_ours(args):
     if os.path.exists(tfile):
         with open(tfile) as f:
             tj = json.load(f)
-        key = args.precision
+        key = f"{args.precision}_kind{tile[2]}"
         if key in tj:
             # ncu DRAM bytes per output site per RHS of the captured launch, scaled to this launch
             traffic = tj[key]["dram_bytes_per_site_rhs"] * (V // 2) * NSRC
@@ -281,9 +280,8 @@ def run_ours(args):
         "data": "synthetic (seeded exp(i eps H) links, point sources)",
         "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, L)), "sources_per_gpu": NSRC,
                    "solver": "even-odd CG, all sources in one batch, CUDA-graph iterations",
-                   "storage": {"half": "fp16 spinors + 12-real fp16 links",
-                               "single": "fp32 spinors + 12-real fp32 links",
-                               "double": "fp64"}[args.precision],
+                   "storage": {"half": "fp16 spinors", "single": "fp32 spinors",
+                               "double": "fp64 spinors"}[args.precision] + " + " + hop_links(args.precision, tile),
                    "accumulate": "fp32 inner, fp64 reliable updates / solution / residual checks",
                    "l2": "inputs larger than L2 (links alone 201 MB fp16, spinor batches > 600 MB)",
                    "parallelism": f"replicas x{world} (independent sources per GPU)"},
@@ -297,7 +295,8 @@ def run_ours(args):
         "e2e": {"value": e2e_s, "unit": "s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "gpu_launches": launches,
         "roofline": {
-            "kernel": (f"{hop_kernel_name(args.precision, tile)}<{args.precision} spinors, 12-real links, "
+            "kernel": (f"{hop_kernel_name(args.precision, tile)}<{args.precision} spinors, "
+                       f"{hop_links(args.precision, tile)}, "
                        f"{NSRC}-RHS batch, {tile[0]} RHS/thread, {tile[1]} threads/block, kind {tile[2]}>"),
             "bound": "hbm",
             "achieved": achieved,
@@ -389,6 +388,22 @@ def _roofline(kernel, launches, ms, nbytes, traffic=None):
             "algorithmic_bytes_per_launch": per}
 
 
+def hop_links(precision, tile):
+    """The link format a sloppy-hop tile reads."""
+    if precision in ("half", "fp16") and tile[2] == 9:
+        return "18-real fp32 links"
+    if precision in ("half", "fp16") and tile[2] in (10, 11):
+        return "18-real fp16 links"
+    return {"half": "12-real fp16 links", "fp16": "12-real fp16 links", "single": "12-real fp32 links",
+            "double": "18-real fp64 links"}[precision]
+
+
+def hop_link_bytes(precision, tile):
+    """Bytes of one link in the format a sloppy-hop tile reads."""
+    return {"12-real fp16 links": 24.0, "18-real fp16 links": 36.0, "12-real fp32 links": 48.0,
+            "18-real fp32 links": 72.0, "18-real fp64 links": 144.0}[hop_links(precision, tile)]
+
+
 def hop_kernel_name(precision, tile):
     """The sloppy hop kernel a tile (rhs_per_thread, threads_per_block, kind) launches."""
     if 1 <= tile[2] <= 3:
@@ -415,12 +430,13 @@ def run_dslash(args):
     Vh = lat.V // 2
     hops = {}
     with ClockSampler(0) as clk:
-        for name, prec, S, G in (("fp16", Q.PREC_HALF, 52.0, 24.0), ("fp32", Q.PREC_SINGLE, 96.0, 48.0)):
+        for name, prec, S in (("fp16", Q.PREC_HALF, 52.0), ("fp32", Q.PREC_SINGLE, 96.0)):
             nr, nt, ms = lat.tune(prec, NSRC)  # CUDA events around 3 pairs of Schur hops per tile, best tile
             table = lat.tune_table(prec, NSRC)
             best = min(table, key=lambda e: e["ms_per_hop"])["tile"]
             # one output parity: input and output spinors, links shared by the batch, the
             # xpay operand on every second hop of the pair
+            G = hop_link_bytes({"fp16": "half", "fp32": "single"}[name], best)
             nbytes = Vh * NSRC * (2.5 * S + 8.0 * G / NSRC)
             hops[name] = {"tile": best, "ms_per_hop": ms, "gbs": nbytes / (ms * 1e-3) / 1e9,
                           "algorithmic_bytes_per_hop": nbytes,
@@ -731,8 +747,6 @@ def main():
     ap.add_argument("--ptc-steps", type=int, default=2000)
     ap.add_argument("--lattice", type=lambda v: tuple(int(x) for x in v.split(",")), default=L,
                     help="X,Y,Z,T for the non-default workloads")
-    ap.add_argument("--fp64-traversal", type=int, default=-1,
-                    help="order of the FP64 hop: -1 automatic, 0 cb order, k>0 chunks of k site blocks")
     ap.add_argument("--tile", type=lambda v: tuple(int(x) for x in v.split(",")), default=None,
                     help="RHS_PER_THREAD,THREADS_PER_BLOCK,KIND of the sloppy hop instead of the autotuner's")
     args = ap.parse_args()

@@ -294,15 +294,6 @@ QKX_API int qkx_tune(qkx_ctx* ctx, int precision, int nrhs, int* rhs_per_thread,
 QKX_API int qkx_set_tile(qkx_ctx* ctx, int precision, int nrhs, int rhs_per_thread, int threads_per_block,
                          int kind);
 
-/* The order in which the FP64 hopping kernel (every FP64 operator, solver
- * and reliable update of this context) walks the lattice; the result is the
- * same in every order.  chunk_blocks = -1 (default): automatic, cb order
- * unless the right-hand sides of a batch make two t-slices larger than L2,
- * then chunks of a t-slice walked chunk by chunk; 0: cb order; k > 0: chunks
- * of k blocks of 64 sites, k dividing the blocks of a t-slice (L0 L1 L2 / 128
- * of them).  No reference counterpart. */
-QKX_API int qkx_set_fp64_traversal(qkx_ctx* ctx, int chunk_blocks);
-
 /* The per-tile timings of the last tuning of (precision, nrhs): *count tiles,
  * the first min(*count, max) written to the arrays (any may be NULL).  0 tiles
  * if that key was never tuned.  No reference counterpart. */

@@ -68,7 +68,7 @@ SYMBOLS = [
     "qkx_host_alloc", "qkx_host_free", "qkx_device_alloc", "qkx_device_free",
     "qkx_memcpy_h2d", "qkx_memcpy_d2h",
     "qkx_profile_enable", "qkx_profile_read", "qkx_profile_reset", "qkx_kernel_launches", "qkx_tune",
-    "qkx_set_tile", "qkx_set_fp64_traversal", "qkx_tune_table", "qkx_sloppy_normal",
+    "qkx_set_tile", "qkx_tune_table", "qkx_sloppy_normal",
     "qkx_plaquette", "qkx_plaquette_loaded", "qkx_project_su3", "qkx_ape_smear", "qkx_load_smearing_gauge",
     "qkx_gaussian_smear", "qkx_gaussian_smear_dev", "qkx_propagator_absorb", "qkx_propagator",
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
@@ -199,7 +199,6 @@ def lib() -> C.CDLL:
         L.qkx_kernel_launches.restype = C.c_longlong
         L.qkx_tune.argtypes = [_vp, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int), _dp]
         L.qkx_set_tile.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int]
-        L.qkx_set_fp64_traversal.argtypes = [_vp, C.c_int]
         L.qkx_tune_table.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), _vp, _vp, _vp, _vp]
         L.qkx_sloppy_normal.argtypes = [_vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(_vp),
                                         C.POINTER(_vp)]
@@ -604,11 +603,6 @@ class Lattice:
         this precision and batch size instead of the tuned one."""
         t = tuple(tile) + (0,) * (3 - len(tile))
         check(lib().qkx_set_tile(self.ctx, precision, nrhs, int(t[0]), int(t[1]), int(t[2])))
-
-    def set_fp64_traversal(self, chunk_blocks: int = -1) -> None:
-        """Order of the FP64 hop over the lattice: -1 automatic (default), 0 cb order, k > 0
-        chunks of k 64-site blocks of a t-slice.  The result is the same in every order."""
-        check(lib().qkx_set_fp64_traversal(self.ctx, int(chunk_blocks)))
 
     def tune_table(self, precision: int = PREC_HALF, nrhs: int = 12) -> list:
         """Every tile timed by the last tuning of (precision, nrhs): dicts with the tile

@@ -135,37 +135,10 @@ static double hop_bytes(size_t nout, double S, double G, bool both, bool extra_x
 // FP64 sites per block of the colour-split kernel (x 3 colour threads)
 constexpr int C3_NS = 64;
 
-// Site-block traversal of the FP64 hop over nrhs right-hand sides (HopArgs::chunk_blocks).
-// A site is read again by its t-1 and t+1 neighbours two t-slices later in cb order,
-// after 2 x (sites of a slice) x nrhs x ~500 B of other traffic: more than L2 holds
-// for a 12-RHS FP64 batch at 32^3x64 (~190 MB), so the grid is walked in chunks of
-// a slice, the largest whose two-slice working set stays within ~48 MB.
-static void hop64_chunks(const qkx_ctx* c, int nrhs, HopArgs<SpinorF64, GaugeF64x18>& A) {
-  A.chunk_blocks = 0;
-  A.slice_blocks = 0;
-  const long S = (long)c->Vh / c->p.L[3];  // cb of one parity in a t-slice
-  if (S % C3_NS || c->fp64_chunk == 0) return;
-  const int sbk = (int)(S / C3_NS);
-  if (c->fp64_chunk > 0) {
-    A.chunk_blocks = c->fp64_chunk;  // checked to divide sbk when it was set
-    A.slice_blocks = sbk;
-    return;
-  }
-  const long budget = 48L << 20;
-  const long per_block = 2L * C3_NS * nrhs * 512;
-  if ((long)sbk * per_block <= budget) return;
-  int best = 1;
-  for (int k = 1; k <= sbk; k++)
-    if (sbk % k == 0 && (long)k * per_block <= budget) best = k;
-  A.chunk_blocks = best;
-  A.slice_blocks = sbk;
-}
-
 // one FP64 18-real hop launch over A.nrhs right-hand sides
 template <int B, bool DAG, int EPI>
 static void launch_hop64(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A) {
   A.nblk = c3_blocks_per_rhs<C3_NS>(c->Vh, A.out_parity);
-  hop64_chunks(c, A.nrhs, A);
   hop_c3_kernel<C3_NS, SpinorF64, B, DAG, EPI><<<A.nblk * A.nrhs, dim3(C3_NS, 3), 0, c->st>>>(A);
   counted(c);
 }
@@ -1031,21 +1004,6 @@ int qkx_set_tile(qkx_ctx* c, int precision, int nrhs, int rhs_per_thread, int th
   if (!c) return invalid("ctx is NULL");
   if (nrhs < 1 || nrhs > MAX_RHS) return invalid("nrhs must be in 1..64");
   return set_tile(c, precision, nrhs, rhs_per_thread, threads_per_block, kind);
-}
-
-int qkx_set_fp64_traversal(qkx_ctx* c, int chunk_blocks) {
-  if (!c) return invalid("ctx is NULL");
-  if (chunk_blocks > 0) {
-    const long S = (long)c->Vh / c->p.L[3];
-    if (S % C3_NS || (S / C3_NS) % chunk_blocks) {
-      set_error("invalid argument: chunk_blocks must divide the %d-site blocks of a t-slice (%ld sites)", C3_NS, S);
-      return QKX_ERR_INVALID;
-    }
-  } else if (chunk_blocks < -1) {
-    return invalid("chunk_blocks must be -1, 0 or positive");
-  }
-  c->fp64_chunk = chunk_blocks;
-  return QKX_OK;
 }
 
 int qkx_tune_table(qkx_ctx* c, int precision, int nrhs, int max, int* count, int* rhs_per_thread,

@@ -45,23 +45,7 @@ struct HopArgs {
   const double* cvec;  // optional per-RHS factor on c (twisted mass per RHS)
   const double* svec;  // optional per-RHS factor on s
   const int* active;   // optional per-RHS mask; inactive blocks do nothing
-  // Site-block traversal (kernels that honour it: hop_c3_kernel).  0: site
-  // blocks in cb order.  > 0: each t-slice's cb range is cut into chunks of
-  // chunk_blocks site blocks, and the grid walks chunk by chunk, t-slice by
-  // t-slice inside a chunk, so a site's t-1 and t+1 users run 2 chunks (not 2
-  // slices) apart and a batch of right-hand sides still finds it in L2.
-  int chunk_blocks = 0;
-  int slice_blocks = 0;  // site blocks per t-slice (a multiple of chunk_blocks)
 };
-
-// traversal index -> site block in cb order (see HopArgs::chunk_blocks)
-__device__ __forceinline__ int chunked_site_block(int sb, int chunk_blocks, int slice_blocks, int Lt) {
-  const int per_chunk = chunk_blocks * Lt;
-  const int chunk = sb / per_chunk;
-  const int r = sb - chunk * per_chunk;
-  const int t = r / chunk_blocks;
-  return t * slice_blocks + chunk * chunk_blocks + (r - t * chunk_blocks);
-}
 
 template <typename R>
 __device__ __forceinline__ void zero(Spinor<R>& s) {

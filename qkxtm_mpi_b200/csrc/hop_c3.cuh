@@ -14,7 +14,6 @@
 //
 // Block: (NS sites) x (3 colours).  Grid: blockIdx.x = site_block * nrhs + rhs;
 // with both parities the site blocks alternate parity (link reuse through L2).
-// Site blocks run in cb order or chunked by t-slice (HopArgs::chunk_blocks).
 #pragma once
 #include "hop.cuh"
 
@@ -90,10 +89,14 @@ __global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18>
     if (slot && threadIdx.x == 0 && threadIdx.y == 0) *slot = 0.0;
     return;
   }
-  int par = A.out_parity < 0 ? blk & 1 : A.out_parity;
-  int sb = A.out_parity < 0 ? blk >> 1 : blk;
-  if (A.chunk_blocks) sb = chunked_site_block(sb, A.chunk_blocks, A.slice_blocks, A.g.L[3]);
-  const int cb = sb * NS + threadIdx.x;
+  int par, cb;
+  if (A.out_parity < 0) {
+    par = blk & 1;
+    cb = (blk >> 1) * NS + threadIdx.x;
+  } else {
+    par = A.out_parity;
+    cb = blk * NS + threadIdx.x;
+  }
   const int a = threadIdx.y;
   double nrm = 0.0;
   if (cb < A.g.Vh) {

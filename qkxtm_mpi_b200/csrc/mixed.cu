@@ -621,10 +621,13 @@ struct Sloppy {
   }
 
   // algorithmic bytes of one of the four inner hops, averaged, per RHS in a batch of R_:
-  // per output site the input and output spinors, 8 links shared by the batch, and
-  // for the two xpay hops one more spinor
-  static double hop_bytes_per_rhs(qkx_ctx* c, int R_) {
-    const double S = P::S, G = P::G, Vh = c->Vh;
+  // per output site the input and output spinors, 8 links shared by the batch in the
+  // tile's link format, and for the two xpay hops one more spinor
+  static double hop_bytes_per_rhs(qkx_ctx* c, int R_, const HopTile& tile) {
+    const double S = P::S, Vh = c->Vh;
+    double G = P::G;
+    if (P::id == QKX_PREC_HALF && tile.kind == 9) G = 72.0;  // 18-real FP32 links
+    if (P::id == QKX_PREC_HALF && (tile.kind == 10 || tile.kind == 11)) G = 36.0;  // 18-real FP16 links
     return Vh * ((2 * S + 8 * G / R_) + (3 * S + 8 * G / R_)) / 2.0;
   }
 };
@@ -929,7 +932,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
         QKX_CUDA(cudaEventElapsedTime(&ms, m->gev[2 * h], m->gev[2 * h + 1]));
         c->prof_ms += ms;
         c->prof_launches++;
-        c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs) * nact;
+        c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs, tile) * nact;
       }
     }
     // reliable update of every active RHS when one of them asks for it

@@ -49,7 +49,6 @@ struct qkx_ctx {
   int compressible = 0;
   int raw_sign = 1;
   double link_unitarity = 0;  // max |U U^+ - 1|
-  int fp64_chunk = -1;        // FP64 hop traversal: -1 auto, 0 cb order, k > 0 chunks of k site blocks
   double2* U18 = nullptr;     // [2][4][9][Vh] FP64, as the operator uses them
   float4* U12f = nullptr;     // [2][4][3][Vh] FP32 12-real, SU(3)
   uint4* U12ha = nullptr;     // [2][4][Vh]  FP16 12-real complex 0..3

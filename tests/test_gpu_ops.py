@@ -203,47 +203,6 @@ def test_invert_fp64_true_residual(qkx, oracle, lattices):
     np.testing.assert_allclose(info.true_residual, tr, rtol=1e-3)
 
 
-@pytest.mark.parametrize("chunk", [0, 1, 2])
-def test_fp64_traversal_matches_oracle(qkx, oracle, chunk):
-    """The FP64 hop walked in cb order (0) or in chunks of 1 or 2 site blocks of a t-slice
-    gives every operator to 1e-13 of the oracle (8^3x16: 4 blocks of 64 sites a slice)."""
-    L = (8, 8, 8, 16)
-    U, psi = _inputs(oracle, L, 0.3, 300, 400)
-    for ts in (1, -1):
-        with qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004, twistSign=ts)) as lat:
-            lat.set_fp64_traversal(chunk)
-            lat.load_gauge(U, qkx.LINKS_AS_GIVEN)
-            for op in oracle.REF_OPS:
-                got = lat.apply(op, psi)
-                exp = oracle.apply(op, L, U, psi, 0.1615, 0.004, ts)
-                assert rel(got, exp) < TOL, (chunk, op, ts, rel(got, exp))
-
-
-@pytest.mark.parametrize("chunk", [0, 1])
-def test_fp64_traversal_in_batched_solve(qkx, oracle, chunk):
-    """The batched FP64 hop of the reliable updates (per-RHS masks, twist factors and norm
-    partials) in either order: each solve reaches the FP64 true residual."""
-    L = (8, 8, 8, 16)
-    U, _ = _inputs(oracle, L, 0.3, 70, 71)
-    bs = [oracle.spinor_gaussian(L, 500 + i) for i in range(3)]
-    with qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004)) as lat:
-        lat.set_fp64_traversal(chunk)
-        lat.load_gauge(U)
-        xs, info = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_SINGLE, tol=1e-10)
-        for b, x in zip(bs, xs):
-            r = b - oracle.apply("tm", L, U, x, 0.1615, 0.004)
-            assert np.sqrt(np.sum(r * r) / np.sum(b * b)) <= 1e-10
-        assert info.true_residual <= 1e-10
-
-
-def test_fp64_traversal_rejects_bad_chunks(qkx):
-    with qkx.Lattice(qkx.LatticeInfo(L=(8, 8, 8, 16))) as lat:
-        for bad in (3, 8, -2):  # 3 does not divide the 4 blocks of a slice, 8 exceeds them
-            with pytest.raises(qkx.QkxError) as e:
-                lat.set_fp64_traversal(bad)
-            assert e.value.code == qkx.ERR_INVALID
-
-
 def test_errors_are_status_codes(qkx, oracle):
     L = (4, 4, 4, 4)
     with qkx.Lattice(qkx.LatticeInfo(L=L)) as lat:
