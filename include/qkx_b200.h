@@ -194,7 +194,9 @@ typedef struct qkx_solve_info {
   int iterations;          /* CG iterations (max over right-hand sides) */
   int reliable_updates;    /* FP64 residual recomputations (mixed precision) */
   int converged;           /* 1 if every right-hand side met its target */
-  int restarts;            /* outer restarts made to reach the true-residual target */
+  int restarts;            /* CG_FP64: outer restarts made to reach the true-residual target;
+                              CG_EO_MIXED: reliable updates after which a search direction
+                              restarted from the new residual (it had grown more than 2x) */
   double true_residual;    /* max over RHS of ||b - M x|| / ||b||, recomputed in FP64 */
   double normal_residual;  /* max over RHS of the final CG residual ||r|| / ||in|| */
   double seconds;          /* device time of the solve (CUDA events) */
@@ -231,7 +233,11 @@ typedef struct qkx_solver_params {
   double tol;              /* target for the true residual ||b - M x|| / ||b|| */
   int maxIter;             /* total iteration cap */
   double reliable_delta;   /* FP64 residual recomputation when |r| drops by this factor;
-                              <= 0 picks the default of the sloppy precision (1e-2 half, 1e-5 single) */
+                              <= 0 picks the default of the sloppy precision (1e-2 half, 1e-5 single);
+                              clamped to [5e-3, 0.5] for half and [1e-7, 0.5] for single: below that
+                              the sloppy recursion drifts from the true residual and the solve
+                              diverges (a right-hand side whose FP64 true residual grows 1000x
+                              above its best is stopped with QKX_ERR_NOT_CONVERGED) */
   int use_graphs;          /* replay the inner iteration from a CUDA graph */
   const double* mu;        /* NULL, or nrhs twisted masses (one per right-hand side, the
                               multi-mass solve of CG_EO_MIXED); NULL = the context's mu */

@@ -135,11 +135,11 @@ static double hop_bytes(size_t nout, double S, double G, bool both, bool extra_x
 // FP64 sites per block of the colour-split kernel (x 3 colour threads)
 constexpr int C3_NS = 64;
 
-// one FP64 18-real hop launch over A.nrhs right-hand sides
+// one FP64 18-real hop launch over A.nrhs right-hand sides (Rz: operands of EPI_XPAY_G5_RES)
 template <int B, bool DAG, int EPI>
-static void launch_hop64(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A) {
+static void launch_hop64(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A, const HopRes& Rz = HopRes{}) {
   A.nblk = c3_blocks_per_rhs<C3_NS>(c->Vh, A.out_parity);
-  hop_c3_kernel<C3_NS, SpinorF64, B, DAG, EPI><<<A.nblk * A.nrhs, dim3(C3_NS, 3), 0, c->st>>>(A);
+  hop_c3_kernel<C3_NS, SpinorF64, B, DAG, EPI><<<A.nblk * A.nrhs, dim3(C3_NS, 3), 0, c->st>>>(A, Rz);
   counted(c);
 }
 
@@ -192,6 +192,29 @@ static int hop64_batch_t(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 out, Spin
   A.svec = svec;
   A.active = active;
   launch_hop64<0, false, EPI>(c, A);
+  QKX_CUDA(cudaGetLastError());
+  if (nblk) *nblk = A.nblk;
+  return QKX_OK;
+}
+
+int hop64_batch_res(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 x, SpinorF64 w, SpinorF32 res32, int out_parity,
+                    double a, double csign, const double* cvec, const int* active, double* norm_part, int* nblk) {
+  HopArgs<SpinorF64, GaugeF64x18> A;
+  A.out = SpinorF64{nullptr, nullptr, c->Vh};
+  A.in = in;
+  A.x = x;
+  A.gauge = GaugeF64x18{c->U18, c->Vh};
+  A.g = c->geom;
+  A.out_parity = out_parity;
+  A.a = a;
+  A.c = csign;
+  A.s = 1.0;
+  A.norm_part = norm_part;
+  A.nrhs = nrhs;
+  A.cvec = cvec;
+  A.svec = nullptr;
+  A.active = active;
+  launch_hop64<0, false, EPI_XPAY_G5_RES>(c, A, HopRes{w, res32});
   QKX_CUDA(cudaGetLastError());
   if (nblk) *nblk = A.nblk;
   return QKX_OK;

@@ -25,6 +25,7 @@ struct CgScalars {
   int iters[MAX_RHS];
   double aux[MAX_RHS];   // per-RHS results of the batched FP64 residual steps
   double aux2[MAX_RHS];
+  int restart[MAX_RHS];  // 1: restart the search direction from the residual (p = r)
 };
 
 template <int NT>

@@ -81,7 +81,7 @@ __device__ __forceinline__ Spin4<double> twist_inv4(const Spin4<double>& v, doub
 }
 
 template <int NS, class SP, int B, bool DAG, int EPI>
-__global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18> A) {
+__global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18> A, HopRes Rz) {
   const int rhs = blockIdx.x % A.nrhs;
   const int blk = blockIdx.x / A.nrhs;
   double* slot = A.norm_part ? A.norm_part + (size_t)rhs * A.nblk + blk : nullptr;
@@ -135,15 +135,31 @@ __global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18>
         const Spin4<double> g5v = gamma5_4<B>(v);
 #pragma unroll
         for (int sp = 0; sp < 4; sp++) o.s[sp] = A.a * acc.s[sp] + (v.s[sp] + c * phase<1>(g5v.s[sp]));
-        if constexpr (EPI == EPI_XPAY_G5) o = gamma5_4<B>(o);
+        if constexpr (EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_RES) o = gamma5_4<B>(o);
       }
     }
-    const SP os = A.out.shift(rhs);
-    double2* ob = (par ? os.p1 : os.p0) + cb;
+    if constexpr (EPI == EPI_XPAY_G5_RES) {
+      // res = w - o in FP64 and its norm; stored as FP32, complex k = sp*3 + a in half k%2
+      // of float4 word k/2
+      const SpinorF64 ws = Rz.w.shift(rhs);
+      const double2* wb = (par ? ws.p1 : ws.p0) + cb;
+      const SpinorF32 rs = Rz.res32.shift(rhs);
+      float2* rb = reinterpret_cast<float2*>((par ? rs.p1 : rs.p0) + cb);
 #pragma unroll
-    for (int sp = 0; sp < 4; sp++) {
-      ob[(size_t)(sp * 3 + a) * Vh] = make_double2(o.s[sp].re, o.s[sp].im);
-      nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
+      for (int sp = 0; sp < 4; sp++) {
+        const Cx<double> z = ldc(wb + (size_t)(sp * 3 + a) * Vh) - o.s[sp];
+        nrm += z.re * z.re + z.im * z.im;
+        const int k = sp * 3 + a;
+        rb[2 * (size_t)(k >> 1) * Vh + (k & 1)] = make_float2(float(z.re), float(z.im));
+      }
+    } else {
+      const SP os = A.out.shift(rhs);
+      double2* ob = (par ? os.p1 : os.p0) + cb;
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) {
+        ob[(size_t)(sp * 3 + a) * Vh] = make_double2(o.s[sp].re, o.s[sp].im);
+        nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
+      }
     }
   }
   if (slot) {

@@ -47,7 +47,9 @@ struct PHalf {
   using GA = GaugeF16x12;
   using R = float;
   using AC = SpinorF32;
-  static constexpr double S = 52.0, G = 24.0, delta = 1e-2;
+  // delta_min: FP16 storage cannot follow the residual much below 1e-3 of its value at the
+  // last update (a 1e-3 threshold diverged on a 32^3x64 batch, 3e-3 converged)
+  static constexpr double S = 52.0, G = 24.0, delta = 1e-2, delta_min = 5e-3;
 };
 struct PSingle {
   static constexpr int id = QKX_PREC_SINGLE;
@@ -55,7 +57,7 @@ struct PSingle {
   using GA = GaugeF32x12;
   using R = float;
   using AC = SpinorF32;
-  static constexpr double S = 96.0, G = 48.0, delta = 1e-5;
+  static constexpr double S = 96.0, G = 48.0, delta = 1e-5, delta_min = 1e-7;
 };
 struct PDouble {
   static constexpr int id = QKX_PREC_DOUBLE;
@@ -63,7 +65,7 @@ struct PDouble {
   using GA = GaugeF64x18;
   using R = double;
   using AC = SpinorF64;
-  static constexpr double S = 192.0, G = 144.0, delta = 1e-30;
+  static constexpr double S = 192.0, G = 144.0, delta = 1e-30, delta_min = 1e-30;
 };
 
 // a batch of single-parity fields: data [R][words][Vh] (+ norms [R][Vh] for FP16)
@@ -742,17 +744,18 @@ static int schur64_g5_batch(qkx_ctx* c, int R_, double csign, double2* v, double
 // the true residual rhat it is built from is FP64, and the sloppy iterations that continue
 // from r round to FP16 or FP32 themselves.  m->r64 is the scratch (the FP32 copy of z and
 // the odd-parity intermediate, 96 B per site and RHS each).
-static int normal_residual_f32(qkx_ctx* c, int R_, double2* z, SpinorF32 out, int* nblk) {
+static SpinorF32 scratch32(qkx_ctx* c, int R_, int which) {
+  using F32 = FieldTraits<SpinorF32>;
+  const BField f{(float4*)c->mixed->r64 + which * F32::words * (size_t)c->Vh * R_, nullptr};
+  return F32::acc(f, which, c->Vh);  // 0: even-parity z32, 1: odd-parity t32
+}
+
+// the same from z = g5 rhat already in FP32 (the even half of the r64 scratch)
+static int normal_residual_from32(qkx_ctx* c, int R_, SpinorF32 out, int* nblk) {
   MixedState* m = c->mixed;
   const int Vh = c->Vh;
   const double k = c->p.kappa;
-  using F32 = FieldTraits<SpinorF32>;
-  const BField zb{m->r64, nullptr}, tb{(float4*)m->r64 + F32::words * (size_t)Vh * R_, nullptr};
-  const SpinorF32 z32 = F32::acc(zb, 0, Vh), t32 = F32::acc(tb, 1, Vh);
-  const dim3 cg2((Vh + 255) / 256, R_);
-  k_mx_from_f64<SpinorF32, float><<<cg2, 256, 0, c->st>>>(B64(z, 0, Vh), z32, c->sc->active);
-  counted(c);
-  QKX_CUDA(cudaGetLastError());
+  const SpinorF32 z32 = scratch32(c, R_, 0), t32 = scratch32(c, R_, 1);
   const GaugeF32x12 U{c->U12f, Vh};
   QKX_TRY((hop_batch<SpinorF32, GaugeF32x12, float, EPI_TWIST_INV>(c, R_, U, c->geom_raw, z32, t32, z32, 1, 0.0,
                                                                    -1.0, true, nullptr, -1)));
@@ -760,6 +763,15 @@ static int normal_residual_f32(qkx_ctx* c, int R_, double2* z, SpinorF32 out, in
                                                                  -1.0, false, m->part, -1)));
   *nblk = hop_blocks_per_rhs<128>(Vh, 0);
   return QKX_OK;
+}
+
+static int normal_residual_f32(qkx_ctx* c, int R_, double2* z, SpinorF32 out, int* nblk) {
+  const int Vh = c->Vh;
+  const dim3 cg2((Vh + 255) / 256, R_);
+  k_mx_from_f64<SpinorF32, float><<<cg2, 256, 0, c->st>>>(B64(z, 0, Vh), scratch32(c, R_, 0), c->sc->active);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  return normal_residual_from32(c, R_, out, nblk);
 }
 
 template <class P>
@@ -779,7 +791,8 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   const size_t n12 = 12 * (size_t)Vh;
   const size_t hb = sizeof(double2) * n12;
   const double k = c->p.kappa, ts = c->p.twistSign;
-  const double delta = sp->reliable_delta > 0 ? std::max(1e-12, std::min(0.5, sp->reliable_delta)) : P::delta;
+  const double delta =
+      sp->reliable_delta > 0 ? std::max(P::delta_min, std::min(0.5, sp->reliable_delta)) : P::delta;
   const int nblk = hop_blocks_per_rhs<128>(Vh, 0);
   const int cgrid = (Vh + 255) / 256;
   const dim3 cg2(cgrid, nrhs), bg2(MX_GRID, nrhs);
@@ -855,10 +868,14 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   QKX_CUDA(cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]));
   bool ru_pending = false;  // a reliable update's end mark not yet read
 
-  std::vector<double> bnorm2(nrhs), r2ru(nrhs), ratio(nrhs, 1.0);
+  // r2rec: the sloppy r^2 when a reliable update was asked for; best: the smallest FP64
+  // true residual ||rhat||^2 seen so far (||b^||^2 at x = 0)
+  std::vector<double> bnorm2(nrhs), r2ru(nrhs), ratio(nrhs, 1.0), r2rec(nrhs, 0.0), best(nrhs);
   std::vector<int> active(nrhs, 1);
+  int diverged = 0;
   for (int i = 0; i < nrhs; i++) {
     bnorm2[i] = sh->aux[i];
+    best[i] = sh->aux2[i];
     r2ru[i] = sh->r2[i];
     ratio[i] = sh->r2[i] > 0 ? sh->aux2[i] / sh->r2[i] : 1.0;  // ||rhat||^2 / ||Mh^+ rhat||^2 at x = 0
     if (bnorm2[i] == 0.0 || sh->r2[i] == 0.0) active[i] = 0;
@@ -906,7 +923,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
 
   const int maxIter = sp->maxIter;
   const double target = 0.9 * sp->tol;
-  int iter = 0, n_ru = 0, since = 0;
+  int iter = 0, n_ru = 0, since = 0, n_restart = 0;
   while (iter < maxIter) {
     int nact = 0;
     for (int i = 0; i < nrhs; i++) nact += active[i];
@@ -944,6 +961,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
         set_error("mixed CG: r2 of right-hand side %d became %g at iteration %d", i, r2s, iter);
         return QKX_ERR_NAN;
       }
+      r2rec[i] = r2s;
       if (r2s < delta * delta * r2ru[i] || r2s * ratio[i] <= target * target * bnorm2[i]) ru = true;
     }
     if (!ru) continue;
@@ -953,14 +971,23 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     // x64 += x_s ; z = g5 b^ - g5 Mh x64 = g5 rhat ; r = Mh^+ rhat
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
     counted(c);
-    QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
-    k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
-    counted(c);
-    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
-    counted(c);
-    if constexpr (r32) {  // straight into the sloppy residual of the RHS that go on
-      QKX_TRY(normal_residual_f32(c, nrhs, m->z64, FA::acc(m->rs, 0, Vh), &nb64));
+    if constexpr (r32) {
+      // the second FP64 hop of Mh x64 forms z = g5 b^ - g5 Mh x64 itself: |z|^2 from the FP64
+      // values, z stored in FP32 for the FP32 Mh^+ that follows (straight into the sloppy residual)
+      QKX_TRY(hop64_batch(c, EPI_TWIST_INV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->x64, 0, Vh), 1, 0.0,
+                          +1.0, m->cvec, m->svec, c->sc->active, nullptr, nullptr));
+      int nbz = 0;
+      QKX_TRY(hop64_batch_res(c, nrhs, B64(m->t64, 1, Vh), B64(m->x64, 0, Vh), B64(m->g5bh, 0, Vh),
+                              scratch32(c, nrhs, 0), 0, -k * k, +1.0, m->cvec, c->sc->active, m->part, &nbz));
+      k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbz, FIN_AUX, c->sc);
+      counted(c);
+      QKX_TRY(normal_residual_from32(c, nrhs, FA::acc(m->rs, 0, Vh), &nb64));
     } else {
+      QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
+      k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
+      counted(c);
+      k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+      counted(c);
       QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb64));
     }
     k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
@@ -968,7 +995,9 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     QKX_CUDA(cudaGetLastError());
     QKX_CUDA(cudaMemcpyAsync(sh->aux, c->sc->aux, 2 * sizeof(double) * MAX_RHS, cudaMemcpyDeviceToHost, c->st));
     QKX_CUDA(cudaStreamSynchronize(c->st));
+    bool any_restart = false;
     for (int i = 0; i < nrhs; i++) {
+      sh->restart[i] = 0;
       if (!active[i]) continue;
       const double rhat2 = sh->aux[i], r2 = sh->aux2[i];
       if (rhat2 <= target * target * bnorm2[i] || r2 == 0.0) {
@@ -976,15 +1005,35 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
         sh->active[i] = 0;
         continue;
       }
+      if (!(rhat2 <= 1e6 * best[i])) {  // the true residual grew 1000x above its best: diverged
+        active[i] = 0;
+        sh->active[i] = 0;
+        diverged++;
+        continue;
+      }
+      best[i] = std::min(best[i], rhat2);
       ratio[i] = rhat2 / r2;
       r2ru[i] = r2;
       sh->r2[i] = r2;
+      // The search direction was built from the sloppy residual.  When the residual that
+      // replaces it is much larger, alpha = r^2 / <p, A p> of the next step would be too,
+      // so the direction restarts from the new residual.
+      if (r2 > 4.0 * r2rec[i]) {
+        sh->restart[i] = 1;
+        any_restart = true;
+      }
     }
     // restart the sloppy residual from the new one for the RHS that go on
     QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
     QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
     if constexpr (!r32) {
       k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
+      counted(c);
+    }
+    if (any_restart) {
+      n_restart++;
+      QKX_CUDA(cudaMemcpyAsync(c->sc->restart, sh->restart, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+      k_mx_convert<AC, SP><<<cg2, 256, 0, c->st>>>(FA::acc(m->rs, 0, Vh), FT::acc(m->p, 0, Vh), c->sc->restart);
       counted(c);
     }
     QKX_CUDA(cudaGetLastError());
@@ -1044,6 +1093,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   if (info) {
     info->iterations = it;
     info->reliable_updates = n_ru;
+    info->restarts = n_restart;
     info->converged = rc == QKX_OK;
     info->true_residual = worst;
     info->normal_residual = 0.0;
@@ -1055,7 +1105,11 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     info->seconds_reliable = ms_ru * 1e-3;
     info->seconds_final = ms_final * 1e-3;
   }
-  if (rc == QKX_ERR_NOT_CONVERGED)
+  if (rc == QKX_ERR_NOT_CONVERGED && diverged)
+    set_error("mixed solve: %d right-hand side(s) diverged (FP64 true residual 1000x above its best) after %d "
+              "iterations; a larger reliable_delta keeps the sloppy recursion closer to the true residual",
+              diverged, iter);
+  else if (rc == QKX_ERR_NOT_CONVERGED)
     set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
   return rc;
 }

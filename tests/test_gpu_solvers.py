@@ -217,3 +217,15 @@ def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
     with pytest.raises(qkx.QkxError) as e:
         lat.set_tile(qkx.PREC_HALF, n, (2, 100, 0))
     assert e.value.code == qkx.ERR_INVALID
+
+
+def test_reliable_delta_below_the_half_precision_limit_is_clamped(qkx, oracle, setup8):
+    """A reliable_delta too small for FP16 storage (1e-3 made a 32^3x64 batch diverge) is
+    raised to the half-precision minimum: the solve converges like the default one."""
+    L, U, lat = setup8
+    bs = [oracle.spinor_gaussian(L, 700 + i) for i in range(2)]
+    xs, info = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_HALF, tol=TOL,
+                          reliable_delta=1e-6)
+    for b, x in zip(bs, xs):
+        assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
+    assert info.converged == 1 and info.true_residual <= TOL
