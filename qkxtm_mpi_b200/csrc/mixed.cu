@@ -160,8 +160,10 @@ constexpr int MX_GRID = 148 * 2;  // blocks per RHS for the streaming kernels
 
 // x_s += alpha p ; r_s -= alpha Ap ; partial |r_s|^2      (one RHS per blockIdx.y)
 template <class SP, class AC, typename R>
-__global__ void __launch_bounds__(MX_NT) k_mx_update_xr(SP p, SP Ap, AC xs, AC rs, const CgScalars* sc,
-                                                        double* part) {
+// r_s -= alpha A p and |r_s|^2 partials.  (x_s += alpha p is done by k_mx_update_p, which
+// reads p anyway: one p read less per site and RHS.)
+template <class SP, class AC, typename R>
+__global__ void __launch_bounds__(MX_NT) k_mx_update_r(SP Ap, AC rs, const CgScalars* sc, double* part) {
   const int r = blockIdx.y;
   double* slot = part + (size_t)r * gridDim.x + blockIdx.x;
   if (!sc->active[r]) {
@@ -169,38 +171,41 @@ __global__ void __launch_bounds__(MX_NT) k_mx_update_xr(SP p, SP Ap, AC xs, AC r
     return;
   }
   const R alpha = R(sc->alpha[r]);
-  const SP pr = p.shift(r), Apr = Ap.shift(r);
-  const AC xr = xs.shift(r), rr = rs.shift(r);
+  const SP Apr = Ap.shift(r);
+  const AC rr = rs.shift(r);
   double acc = 0.0;
-  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < p.Vh; cb += gridDim.x * MX_NT) {
-    Spinor<R> pv = pr.load(0, cb), av = Apr.load(0, cb), xv = xr.load(0, cb), rv = rr.load(0, cb);
+  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < Ap.Vh; cb += gridDim.x * MX_NT) {
+    Spinor<R> av = Apr.load(0, cb), rv = rr.load(0, cb);
 #pragma unroll
     for (int k = 0; k < 12; k++) {
-      Cx<R>& X = xv.c[k / 3][k % 3];
       Cx<R>& Q = rv.c[k / 3][k % 3];
-      X = X + alpha * pv.c[k / 3][k % 3];
       Q = Q - alpha * av.c[k / 3][k % 3];
       acc += double(Q.re) * double(Q.re) + double(Q.im) * double(Q.im);
     }
-    xr.store(0, cb, xv);
     rr.store(0, cb, rv);
   }
   double s = block_sum<MX_NT>(acc);
   if (threadIdx.x == 0) *slot = s;
 }
 
-// p = r_s + beta p
+// x_s += alpha p, then p = r_s + beta p (alpha of this iteration, beta from the new r_s)
 template <class SP, class AC, typename R>
-__global__ void __launch_bounds__(MX_NT) k_mx_update_p(SP p, AC rs, const CgScalars* sc) {
+__global__ void __launch_bounds__(MX_NT) k_mx_update_p(SP p, AC xs, AC rs, const CgScalars* sc) {
   const int r = blockIdx.y;
   if (!sc->active[r]) return;
+  const R alpha = R(sc->alpha[r]);
   const R beta = R(sc->beta[r]);
   const SP pr = p.shift(r);
-  const AC rr = rs.shift(r);
+  const AC xr = xs.shift(r), rr = rs.shift(r);
   for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < p.Vh; cb += gridDim.x * MX_NT) {
-    Spinor<R> pv = pr.load(0, cb), rv = rr.load(0, cb);
+    Spinor<R> pv = pr.load(0, cb), rv = rr.load(0, cb), xv = xr.load(0, cb);
 #pragma unroll
-    for (int k = 0; k < 12; k++) pv.c[k / 3][k % 3] = rv.c[k / 3][k % 3] + beta * pv.c[k / 3][k % 3];
+    for (int k = 0; k < 12; k++) {
+      Cx<R>& X = xv.c[k / 3][k % 3];
+      X = X + alpha * pv.c[k / 3][k % 3];
+      pv.c[k / 3][k % 3] = rv.c[k / 3][k % 3] + beta * pv.c[k / 3][k % 3];
+    }
+    xr.store(0, cb, xv);
     pr.store(0, cb, pv);
   }
 }
@@ -612,11 +617,11 @@ struct Sloppy {
     QKX_TRY((hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr,
                                               prof ? 3 : -1)));
     dim3 gr(MX_GRID, R_);
-    k_mx_update_xr<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, Ap, xs, rs, c->sc, m->part);
+    k_mx_update_r<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(Ap, rs, c->sc, m->part);
     counted(c);
     k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, MX_GRID, FIN_R2, c->sc);
     counted(c);
-    k_mx_update_p<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, rs, c->sc);
+    k_mx_update_p<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, xs, rs, c->sc);
     counted(c);
     QKX_CUDA(cudaGetLastError());
     return QKX_OK;
@@ -757,11 +762,13 @@ static int normal_residual_from32(qkx_ctx* c, int R_, SpinorF32 out, int* nblk) 
   const double k = c->p.kappa;
   const SpinorF32 z32 = scratch32(c, R_, 0), t32 = scratch32(c, R_, 1);
   const GaugeF32x12 U{c->U12f, Vh};
-  QKX_TRY((hop_batch<SpinorF32, GaugeF32x12, float, EPI_TWIST_INV>(c, R_, U, c->geom_raw, z32, t32, z32, 1, 0.0,
-                                                                   -1.0, true, nullptr, -1)));
-  QKX_TRY((hop_batch<SpinorF32, GaugeF32x12, float, EPI_XPAY_G5>(c, R_, U, c->geom_raw, t32, out, z32, 0, -k * k,
-                                                                 -1.0, false, m->part, -1)));
-  *nblk = hop_blocks_per_rhs<128>(Vh, 0);
+  // the FP32 batch hop's tile with one RHS a thread and 64 threads (the tuner's choice for
+  // FP32 at 12 RHS on 24^3x48 and 32^3x64)
+  QKX_TRY((launch_mrhs<64, 1, 0, SpinorF32, GaugeF32x12, float, EPI_TWIST_INV>(c, R_, U, c->geom_raw, z32, t32, z32,
+                                                                                1, 0.0, -1.0, true, nullptr, -1)));
+  QKX_TRY((launch_mrhs<64, 1, 0, SpinorF32, GaugeF32x12, float, EPI_XPAY_G5>(c, R_, U, c->geom_raw, t32, out, z32, 0,
+                                                                              -k * k, -1.0, false, m->part, -1)));
+  *nblk = mrhs_site_blocks<64>(Vh);
   return QKX_OK;
 }
 
