@@ -158,10 +158,8 @@ static void bfield_free(BField& f) {
 constexpr int MX_NT = 256;
 constexpr int MX_GRID = 148 * 2;  // blocks per RHS for the streaming kernels
 
-// x_s += alpha p ; r_s -= alpha Ap ; partial |r_s|^2      (one RHS per blockIdx.y)
-template <class SP, class AC, typename R>
-// r_s -= alpha A p and |r_s|^2 partials.  (x_s += alpha p is done by k_mx_update_p, which
-// reads p anyway: one p read less per site and RHS.)
+// r_s -= alpha A p and |r_s|^2 partials, one RHS per blockIdx.y.  (x_s += alpha p is done by
+// k_mx_update_p, which reads p anyway: one p read less per site and RHS.)
 template <class SP, class AC, typename R>
 __global__ void __launch_bounds__(MX_NT) k_mx_update_r(SP Ap, AC rs, const CgScalars* sc, double* part) {
   const int r = blockIdx.y;
