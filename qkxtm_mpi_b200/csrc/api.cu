@@ -198,7 +198,8 @@ static int hop64_batch_t(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 out, Spin
 }
 
 int hop64_batch_res(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 x, SpinorF64 w, SpinorF32 res32, int out_parity,
-                    double a, double csign, const double* cvec, const int* active, double* norm_part, int* nblk) {
+                    double a, double csign, const double* cvec, const int* active, double* norm_part, int* nblk,
+                    bool g5) {
   HopArgs<SpinorF64, GaugeF64x18> A;
   A.out = SpinorF64{nullptr, nullptr, c->Vh};
   A.in = in;
@@ -214,7 +215,8 @@ int hop64_batch_res(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 x, SpinorF64 w
   A.cvec = cvec;
   A.svec = nullptr;
   A.active = active;
-  launch_hop64<0, false, EPI_XPAY_G5_RES>(c, A, HopRes{w, res32});
+  if (g5) launch_hop64<0, false, EPI_XPAY_G5_RES>(c, A, HopRes{w, res32});
+  else launch_hop64<0, false, EPI_XPAY_RES>(c, A, HopRes{w, res32});
   QKX_CUDA(cudaGetLastError());
   if (nblk) *nblk = A.nblk;
   return QKX_OK;

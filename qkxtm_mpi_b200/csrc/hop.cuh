@@ -29,10 +29,12 @@ enum Epilogue {
   EPI_TWIST_INV = 3,   // out = s (v - i c g5 v), v = D psi      (A^-1 D, first step of tm_xx)
   EPI_XPAY_TWINV = 4,  // out = s (v - i c g5 v), v = a D psi + x (odd-parity reconstruction)
   EPI_XPAY_G5_RES = 5, // res = w - g5 (a D psi + x + i c g5 x), stored in FP32 (hop_c3_kernel only)
+  EPI_XPAY_RES = 6,    // res = w - (a D psi + x + i c g5 x), its norm only (hop_c3_kernel only)
 };
 
-// extra operands of EPI_XPAY_G5_RES: w, and the FP32 field the residual goes to (the
-// output's parity); |res|^2 is summed from the FP64 values before they are rounded
+// extra operands of EPI_XPAY_G5_RES / EPI_XPAY_RES: w, and the FP32 field the residual
+// goes to (the output's parity; a null pointer stores nothing); |res|^2 is summed from
+// the FP64 values before they are rounded
 struct HopRes {
   SpinorF64 w;
   SpinorF32 res32;

@@ -138,19 +138,20 @@ __global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18>
         if constexpr (EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_RES) o = gamma5_4<B>(o);
       }
     }
-    if constexpr (EPI == EPI_XPAY_G5_RES) {
-      // res = w - o in FP64 and its norm; stored as FP32, complex k = sp*3 + a in half k%2
-      // of float4 word k/2
+    if constexpr (EPI == EPI_XPAY_G5_RES || EPI == EPI_XPAY_RES) {
+      // res = w - o in FP64 and its norm; stored (when a target is given) as FP32, complex
+      // k = sp*3 + a in half k%2 of float4 word k/2
       const SpinorF64 ws = Rz.w.shift(rhs);
       const double2* wb = (par ? ws.p1 : ws.p0) + cb;
       const SpinorF32 rs = Rz.res32.shift(rhs);
-      float2* rb = reinterpret_cast<float2*>((par ? rs.p1 : rs.p0) + cb);
+      float4* rq = par ? rs.p1 : rs.p0;
+      float2* rb = rq ? reinterpret_cast<float2*>(rq + cb) : nullptr;
 #pragma unroll
       for (int sp = 0; sp < 4; sp++) {
         const Cx<double> z = ldc(wb + (size_t)(sp * 3 + a) * Vh) - o.s[sp];
         nrm += z.re * z.re + z.im * z.im;
         const int k = sp * 3 + a;
-        rb[2 * (size_t)(k >> 1) * Vh + (k & 1)] = make_float2(float(z.re), float(z.im));
+        if (rb) rb[2 * (size_t)(k >> 1) * Vh + (k & 1)] = make_float2(float(z.re), float(z.im));
       }
     } else {
       const SP os = A.out.shift(rhs);

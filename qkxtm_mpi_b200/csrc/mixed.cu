@@ -983,7 +983,8 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
                           +1.0, m->cvec, m->svec, c->sc->active, nullptr, nullptr));
       int nbz = 0;
       QKX_TRY(hop64_batch_res(c, nrhs, B64(m->t64, 1, Vh), B64(m->x64, 0, Vh), B64(m->g5bh, 0, Vh),
-                              scratch32(c, nrhs, 0), 0, -k * k, +1.0, m->cvec, c->sc->active, m->part, &nbz));
+                              scratch32(c, nrhs, 0), 0, -k * k, +1.0, m->cvec, c->sc->active, m->part, &nbz,
+                              true));
       k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbz, FIN_AUX, c->sc);
       counted(c);
       QKX_TRY(normal_residual_from32(c, nrhs, FA::acc(m->rs, 0, Vh), &nb64));
@@ -1068,16 +1069,13 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
   // x_o = A^-1 (b_o + k D_oe x_e) into t64
   QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
                       m->cvec, m->svec, c->sc->active, nullptr, nullptr));
-  // M x on the full lattice (even half in x64, odd half in t64) into (z64, r64)
-  QKX_TRY(hop64_batch(c, EPI_XPAY, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->z64, m->r64, Vh),
-                      B64full(m->x64, m->t64, Vh), -1, -k, 1.0, m->cvec, nullptr, c->sc->active, nullptr, nullptr));
-  k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), B64(m->z64, 0, Vh), nullptr, m->part);
-  counted(c);
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
-  counted(c);
-  k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), B64(m->r64, 0, Vh), nullptr, m->part);
-  counted(c);
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+  // ||b - M x||^2 on the full lattice (x: even half in x64, odd half in t64), summed in FP64 by the
+  // hop's epilogue; nothing is stored
+  int nbr = 0;
+  QKX_TRY(hop64_batch_res(c, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->x64, m->t64, Vh),
+                          B64full(m->bE, m->bO, Vh), SpinorF32{nullptr, nullptr, Vh}, -1, -k, 1.0, m->cvec,
+                          c->sc->active, m->part, &nbr, false));
+  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbr, FIN_AUX, c->sc);
   counted(c);
   QKX_CUDA(cudaGetLastError());
   for (int i = 0; i < nrhs; i++) {

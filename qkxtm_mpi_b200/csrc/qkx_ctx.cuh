@@ -128,10 +128,12 @@ int hop64a(qkx_ctx* c, int basis, bool dag, int epi, SpinorF64 in, SpinorF64 out
 int hop64_batch(qkx_ctx* c, int epi, int nrhs, SpinorF64 in, SpinorF64 out, SpinorF64 x, int out_parity, double a,
                 double csign, const double* cvec, const double* svec, const int* active, double* norm_part,
                 int* nblk);
-// batched FP64 hop with the EPI_XPAY_G5_RES epilogue: res32(rhs) = w - g5 (a D in + x + i c g5 x) in
-// FP32 on out_parity, |res|^2 partials (FP64) per RHS into norm_part (*nblk of them)
+// batched FP64 hop with a residual epilogue: res32(rhs) = w - g5 (a D in + x + i c g5 x) (g5, EPI_XPAY_G5_RES)
+// or w - (a D in + x + i c g5 x) (EPI_XPAY_RES) in FP32 on out_parity (-1: both; a null res32 stores
+// nothing), |res|^2 partials (FP64) per RHS into norm_part (*nblk of them)
 int hop64_batch_res(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 x, SpinorF64 w, SpinorF32 res32, int out_parity,
-                    double a, double csign, const double* cvec, const int* active, double* norm_part, int* nblk);
+                    double a, double csign, const double* cvec, const int* active, double* norm_part, int* nblk,
+                    bool g5);
 // site-local operator (site_ops.cuh) on parities [par_first, par_first + npar)
 int site_op_acc(qkx_ctx* c, int basis, int op, SpinorF64 in, SpinorF64 out, int par_first, int npar, double cc,
                 double s);
