@@ -229,3 +229,18 @@ def test_reliable_delta_below_the_half_precision_limit_is_clamped(qkx, oracle, s
     for b, x in zip(bs, xs):
         assert true_res(oracle, L, U, x, b, 0.1615, 0.004) <= TOL
     assert info.converged == 1 and info.true_residual <= TOL
+
+
+def test_solve_info_phases(qkx, oracle, setup8):
+    """CG_EO_MIXED reports the device time of its set-up, reliable updates and final residual,
+    each inside the solve's total; the plain FP64 method leaves them zero."""
+    L, U, lat = setup8
+    bs = [oracle.spinor_gaussian(L, 800 + i) for i in range(3)]
+    _, info = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=qkx.PREC_HALF, tol=TOL)
+    parts = (info.seconds_setup, info.seconds_reliable, info.seconds_final)
+    assert all(t > 0 for t in parts), parts
+    assert sum(parts) < info.seconds
+    assert info.reliable_updates >= 1 and info.restarts >= 0
+    _, info64 = lat.invert(bs[:1], method=qkx.SOLVER_CG_FP64, tol=TOL)
+    assert (info64.seconds_setup, info64.seconds_reliable, info64.seconds_final) == (0.0, 0.0, 0.0)
+    assert info64.seconds > 0
