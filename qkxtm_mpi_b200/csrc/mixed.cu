@@ -426,40 +426,6 @@ static int mixed_alloc(qkx_ctx* c, int R, bool solver) {
   return QKX_OK;
 }
 
-// ---------------------------------------------------------------- batched hop launcher
-// EPI as in hop.cuh; csign multiplies the per-RHS twist coefficient cvec; with
-// with_s the per-RHS svec scales TWIST_INV epilogues.
-template <class SP, class GA, typename R, int EPI>
-static int hop_batch(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in, SP out, SP x, int out_parity,
-                     double a, double csign, bool with_s, double* norm_part, int prof_slot) {
-  MixedState* m = c->mixed;
-  HopArgs<SP, GA> A;
-  A.out = out;
-  A.in = in;
-  A.x = x;
-  A.gauge = gauge;
-  A.g = g;
-  A.out_parity = out_parity;
-  A.a = a;
-  A.c = csign;
-  A.s = 1.0;
-  A.norm_part = norm_part;
-  A.nrhs = R_;
-  A.nblk = hop_blocks_per_rhs<128>(c->Vh, out_parity);
-  A.cvec = m->cvec;
-  A.svec = with_s ? m->svec : nullptr;
-  A.active = c->sc->active;
-  if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
-  {
-    hop_kernel<128, SP, GA, R, 0, false, EPI><<<A.nblk * R_, 128, 0, c->st>>>(A);
-    counted(c);
-  }
-  QKX_CUDA(cudaGetLastError());
-  if (prof_slot >= 0)
-    QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot + 1], c->st, cudaEventRecordExternal));
-  return QKX_OK;
-}
-
 // ---------------------------------------------------------------- multi-RHS sloppy hop
 // Tile of the sloppy hop: NR right-hand sides per thread, NT threads per block,
 // and the kernel kind.  Kind 0: hop_mrhs_kernel, or for FP16 with NR even the
