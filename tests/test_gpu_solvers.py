@@ -190,22 +190,24 @@ def test_sloppy_normal_operator_every_tile(qkx, oracle, setup8, prec, tol):
         assert e.value.code == qkx.ERR_INVALID
 
 
-@pytest.mark.parametrize("tile", [(1, 128, 0), (2, 64, 0), (2, 256, 0), (3, 64, 0), (4, 128, 0), (2, 128, 1),
-                                  (2, 256, 2), (2, 64, 3), (2, 128, 4), (2, 128, 5), (2, 64, 6), (2, 64, 7),
-                                  (2, 64, 8), (2, 128, 9), (2, 64, 10), (2, 128, 11)])
-def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, tile):
+@pytest.mark.parametrize("prec,tile", [("half", t) for t in (
+    (1, 128, 0), (2, 64, 0), (2, 256, 0), (3, 64, 0), (4, 128, 0), (2, 128, 1), (2, 256, 2), (2, 64, 3), (2, 128, 4),
+    (2, 128, 5), (2, 64, 6), (2, 64, 7), (2, 64, 8), (2, 128, 9), (2, 64, 10), (2, 128, 11))] + [
+    ("single", (1, 64, 0)), ("single", (2, 128, 0))])
+def test_every_tile_solves_a_multi_mass_batch(qkx, oracle, setup8, prec, tile):
     """Solves with the tile forced: three masses in a batch of five, so right-hand sides
     leave the batch at different iterations (the per-RHS active mask) and the last
     group of the tile is partly outside the batch."""
     import ctypes as C
     L, U, lat = setup8
+    p = {"half": qkx.PREC_HALF, "single": qkx.PREC_SINGLE}[prec]
     mus = [0.0015, 0.01, 0.004, 0.02, 0.0015]
     bs = [oracle.spinor_gaussian(L, 90 + i) for i in range(5)]
     xs = [np.empty_like(b) for b in bs]
     n = len(bs)
-    lat.set_tile(qkx.PREC_HALF, n, tile)
+    lat.set_tile(p, n, tile)
     arr = (C.c_double * n)(*mus)
-    sp = qkx.SolverParams(qkx.SOLVER_CG_EO_MIXED, qkx.PREC_HALF, TOL, 10000, 0.0, 1,
+    sp = qkx.SolverParams(qkx.SOLVER_CG_EO_MIXED, p, TOL, 10000, 0.0, 1,
                           C.cast(arr, C.POINTER(C.c_double)))
     info = qkx.SolveInfo()
     bp = (C.c_void_p * n)(*[b.ctypes.data for b in bs])
