@@ -94,3 +94,45 @@ def test_cpp_dropin_header_compiles():
     """include/qkxTM_b200.hpp (the reference-named C++ layer) is valid C++17."""
     src = os.path.join(ROOT, "tests", "cpp", "test_dropin.cpp")
     subprocess.run(["g++", "-std=c++17", "-fsyntax-only", "-I", os.path.join(ROOT, "include"), src], check=True)
+
+
+# C structs of include/qkx_b200.h and their ctypes mirrors in the Python binding
+_STRUCTS = {
+    "qkx_params": "Params",
+    "qkx_solve_info": "SolveInfo",
+    "qkx_solver_params": "SolverParams",
+    "qkx_batch_job": "BatchJob",
+    "qkx_lime_info": "LimeInfo",
+    "qkx_ptc_params": "PtcParams",
+    "qkx_ptc_train_params": "PtcTrainParams",
+    "qkx_ptc_train_info": "PtcTrainInfo",
+}
+
+
+def test_struct_layouts_match_the_header(tmp_path):
+    """Every ctypes structure of the binding has the size and field offsets of its C struct,
+    as a C compiler lays it out from the header (a mismatch would shift the fields that
+    follow, e.g. the status and message of a batch job after its solve info)."""
+    import qkxtm_mpi_b200 as Q
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "qkx_b200.h"', "int main(void) {"]
+    for cname, pyname in _STRUCTS.items():
+        cls = getattr(Q, pyname)
+        lines.append(f'  printf("{cname} size %zu\\n", sizeof({cname}));')
+        for field, _ in cls._fields_:
+            lines.append(f'  printf("{cname} {field} %zu\\n", offsetof({cname}, {field}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layouts.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layouts"
+    subprocess.run(["gcc", "-std=c11", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n")
+    got = {}
+    for line in out:
+        if line:
+            name, key, val = line.split()
+            got[(name, key)] = int(val)
+    for cname, pyname in _STRUCTS.items():
+        cls = getattr(Q, pyname)
+        assert got[(cname, "size")] == C.sizeof(cls), (cname, got[(cname, "size")], C.sizeof(cls))
+        for field, _ in cls._fields_:
+            assert got[(cname, field)] == getattr(cls, field).offset, (cname, field)
