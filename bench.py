@@ -1,7 +1,7 @@
 #!/usr/bin/env python
 """Benchmark of the twisted-mass Dslash / CG hot path on B200.
 
-Workload (the north-star configuration): 32^3 x 64 lattice, synthetic links
+Workload (the 12-source multi-RHS solve): 32^3 x 64 lattice, synthetic links
 U = exp(i 0.3 H) (seeded), antiperiodic time boundary, kappa = 0.1615,
 mu = 0.0015, the 12 spin-colour point sources at the origin, every source
 solved to a true residual ||b - M x|| / ||b|| <= 1e-10 recomputed in FP64.
