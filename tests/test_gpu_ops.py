@@ -1,6 +1,6 @@
 """GPU parity of the FP64 operators, BLAS, link generator and the reference CG
 against the oracle and the reference's golden vectors, through the C ABI.
-FP64 tolerance: 1e-13 relative (north-star bar for Dslash)."""
+FP64 tolerance: 1e-13 relative (the parity bar for the FP64 operators)."""
 import os
 
 import numpy as np
