@@ -19,11 +19,13 @@
 //   y_e  = g5 (A(c) p_e - k^2 D_eo t_o)        hop, XPAY_G5, |y|^2 = <p, Mh^+Mh p> fused
 //   t_o  = A^-1(-c) D_oe y_e                  hop, TWIST_INV
 //   Ap_e = g5 (A(-c) y_e - k^2 D_eo t_o)       hop, XPAY_G5
-//   alpha = r2 / pAp ; x_s += alpha p ; r_s -= alpha Ap ; r2' = |r_s|^2 ; beta ; p = r_s + beta p
+//   alpha = r2 / pAp ; r_s -= alpha Ap ; r2' = |r_s|^2 ; beta ; x_s += alpha p ; p = r_s + beta p
 // p, t, y, Ap are sloppy (FP16 + per-site norm, or FP32); r_s and x_s are FP32.
 // A reliable update (all active right-hand sides together, so the FP64 hops
-// share the links) folds x_s into the FP64 solution and recomputes the
-// residual with the FP64 operator on the 18-real links as the caller gave them.
+// share the links) folds x_s into the FP64 solution and recomputes the true
+// residual rhat = b^ - Mh x with the FP64 operator on the 18-real links as the
+// caller gave them; the residual the sloppy CG restarts from, Mh^+ rhat, is
+// built from rhat in FP32.
 #include <math.h>
 #include <string.h>
 
