@@ -276,7 +276,9 @@ def run_ours(args):
         "higher_is_better": False,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32",
+        "dtype": {"half": "f16 storage / f32 accumulate / f64 reliable updates, solution and residual",
+                  "single": "f32 storage / f32 accumulate / f64 reliable updates, solution and residual",
+                  "double": "f64"}[args.precision],
         "data": "synthetic (seeded exp(i eps H) links, point sources)",
         "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, L)), "sources_per_gpu": NSRC,
                    "solver": "even-odd CG, all sources in one batch, CUDA-graph iterations",
@@ -331,11 +333,10 @@ def run_reference(args):
 
     O.build(ref=True)
     links = O.apply_bc(L, O.gauge_random(L, EPS, SEED), -1)
-    # iterations of the reference's own stopping rule, from a small lattice
-    iters = CB.iterations_to_converge((8, 8, 8, 16), KAPPA, MU, EPS, SEED)
+    # iterations of the reference's CG recurrence to a true residual of 1e-10, from a small lattice
     vals, last = [], None
     for i in range(args.warmup + args.steps):
-        last = CB.run(L, KAPPA, MU, EPS, SEED, n_sources=NSRC, n_iter=1, iters_full=iters, links=links)
+        last = CB.run(L, KAPPA, MU, EPS, SEED, n_sources=NSRC, n_iter=1, iters_full=None, links=links)
         if i >= args.warmup:
             vals.append(last["value"])
     value = statistics.median(vals)

@@ -181,10 +181,15 @@ QKX_API int qkx_norm2(qkx_ctx* ctx, const double* x_dev, double* result);
  * It calls no cudaMalloc/cudaFree: its scratch (the per-block partial sums)
  * is a fixed 512 KB array compiled into the library, resident on every GPU
  * that loads it until the process exits.  Inputs above QKX_NOALLOC_MAX_SITES
- * sites are rejected with QKX_ERR_INVALID.  The first call on a device looks
- * up the array's device address (cudaGetSymbolAddress), so make that first
- * call before any stream capture.  All calls on a device share the array:
- * calls whose GPU work overlaps (other streams or host threads) race. */
+ * sites are rejected with QKX_ERR_INVALID, and so are field pointers that are
+ * not 16-byte aligned or not device (or managed) memory of the current device,
+ * before anything is launched.  The first call on a device looks up the
+ * array's device address (cudaGetSymbolAddress) and keeps it; after a
+ * cudaDeviceReset of that device the kept address is stale, so do not call
+ * again in that process.  The call waits for its result (a synchronizing copy
+ * to host memory), so it cannot be made on a capturing stream: it returns
+ * QKX_ERR_INVALID there.  All calls on a device share the array: calls whose
+ * GPU work overlaps (other streams or host threads) race. */
 #define QKX_NOALLOC_MAX_SITES 11184810ULL
 QKX_API int qkx_reCdotXdagY_noalloc(const double* x_dev, const double* y_dev, size_t n_sites, double* result,
                                     void* stream);

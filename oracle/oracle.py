@@ -21,7 +21,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "liboracle.so")
 REF_SO = os.path.join(HERE, "_ref", "libqkxref.so")
-REF_SRC = "/root/reference"
+# where the reference sources lie (only the build of the pin and the fixture script read them)
+REF_SRC = os.environ.get("QKX_REFERENCE_SRC", "/root/reference")
 
 UKQCD, CHIRAL = 0, 1
 EO, OE, OO, EE = 0, 1, 2, 3

@@ -73,7 +73,9 @@ int lime_scan(FILE* f, std::vector<LimeRecord>& recs) {
     memcpy(t, h + 16, 128);
     t[128] = 0;
     r.type = t;
-    if (r.offset + r.bytes > size) return bad("LIME record '%s' runs past the end of the file", r.type.c_str());
+    // r.offset <= size here, so size - r.offset cannot wrap; once r.bytes fits,
+    // its 8-byte padded length cannot overflow either
+    if (r.bytes > size - r.offset) return bad("LIME record '%s' runs past the end of the file", r.type.c_str());
     recs.push_back(r);
     pos = r.offset + ((r.bytes + 7) & ~(uint64_t)7);
   }
@@ -222,23 +224,34 @@ int qkx_write_gauge_lime(qkx_ctx* c, const char* path, const double* U_host, con
   const size_t bytes = nwords * 8;
   double* aos = nullptr;
   unsigned long long* be = nullptr;
-  QKX_CUDA(cudaMallocAsync((void**)&aos, bytes, c->st));
-  QKX_CUDA(cudaMallocAsync((void**)&be, bytes, c->st));
-  if (U_host) {
-    QKX_CUDA(cudaMemcpyAsync(aos, U_host, bytes, cudaMemcpyHostToDevice, c->st));
-  } else {
-    k_gauge_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->U18, (double2*)aos, c->geom);
-    counted(c);
-  }
-  // native -> big-endian: the same byte reversal
-  k_bswap64<<<swap_grid(nwords), 256, 0, c->st>>>((const unsigned long long*)aos, (double*)be, nwords);
-  counted(c);
-  QKX_CUDA(cudaGetLastError());
   std::vector<unsigned char> host(bytes);
-  QKX_CUDA(cudaMemcpyAsync(host.data(), be, bytes, cudaMemcpyDeviceToHost, c->st));
-  QKX_CUDA(cudaFreeAsync(aos, c->st));
-  QKX_CUDA(cudaFreeAsync(be, c->st));
-  QKX_CUDA(cudaStreamSynchronize(c->st));
+  // every step runs only if the ones before it succeeded; both buffers are freed on every path
+  cudaError_t e = cudaMallocAsync((void**)&aos, bytes, c->st);
+  if (e == cudaSuccess) e = cudaMallocAsync((void**)&be, bytes, c->st);
+  if (e == cudaSuccess) {
+    if (U_host) {
+      e = cudaMemcpyAsync(aos, U_host, bytes, cudaMemcpyHostToDevice, c->st);
+    } else {
+      k_gauge_eo_to_aos<<<(unsigned)((c->V + 255) / 256), 256, 0, c->st>>>(c->U18, (double2*)aos, c->geom);
+      counted(c);
+      e = cudaGetLastError();
+    }
+  }
+  if (e == cudaSuccess) {
+    // native -> big-endian: the same byte reversal
+    k_bswap64<<<swap_grid(nwords), 256, 0, c->st>>>((const unsigned long long*)aos, (double*)be, nwords);
+    counted(c);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(host.data(), be, bytes, cudaMemcpyDeviceToHost, c->st);
+  if (aos) cudaFreeAsync(aos, c->st);
+  if (be) cudaFreeAsync(be, c->st);
+  const cudaError_t es = cudaStreamSynchronize(c->st);
+  if (e == cudaSuccess) e = es;
+  if (e != cudaSuccess) {
+    set_error("LIME write: %s", cudaGetErrorString(e));
+    return QKX_ERR_CUDA;
+  }
 
   char xml[1024];
   snprintf(xml, sizeof xml,

@@ -14,6 +14,8 @@
 // Every call on a device shares the one array: each call writes all the
 // partials it later reads, so nothing has to be cleared, but calls whose GPU
 // work overlaps (different streams, or different host threads) race on it.
+#include <stdint.h>
+
 #include <mutex>
 
 #include "blas.cuh"
@@ -31,6 +33,8 @@ constexpr int NA_MAX_DEVICES = 64;
 // [0, NA_MAX_BLOCKS): partial sums, one per block; [NA_MAX_BLOCKS]: the result
 static __device__ __align__(256) double g_noalloc_scratch[NA_MAX_BLOCKS + 1];
 
+// the array's device address per device, looked up once; a cudaDeviceReset of a
+// device invalidates it, so a process that resets a device must not call again
 std::mutex g_na_mu;
 double* g_na_ptr[NA_MAX_DEVICES] = {};
 
@@ -59,6 +63,34 @@ __global__ void __launch_bounds__(1024) k_na_final(double* __restrict__ part, in
   if (threadIdx.x == 0) part[NA_MAX_BLOCKS] = s;
 }
 
+// A field pointer the kernel may read: 16-byte aligned (the kernel reads double2)
+// and device or managed memory that the current device `dev` can address.
+// Host memory, registered or not, is refused: reading it from the kernel would
+// fault the GPU or read across PCIe.  cudaPointerGetAttributes allocates nothing.
+bool na_field_ok(const void* p, int dev, const char* name) {
+  if (((uintptr_t)p & 15u) != 0) {
+    qkx::set_error("invalid argument: %s is not 16-byte aligned", name);
+    return false;
+  }
+  cudaPointerAttributes a{};
+  const cudaError_t e = cudaPointerGetAttributes(&a, p);
+  if (e != cudaSuccess) {
+    cudaGetLastError();  // the query records its (non-sticky) error; clear it
+    qkx::set_error("invalid argument: %s is not a CUDA pointer (%s)", name, cudaGetErrorString(e));
+    return false;
+  }
+  if (a.type == cudaMemoryTypeManaged) return true;
+  if (a.type != cudaMemoryTypeDevice) {
+    qkx::set_error("invalid argument: %s is not device memory", name);
+    return false;
+  }
+  if (a.device != dev) {
+    qkx::set_error("invalid argument: %s lives on device %d, the current device is %d", name, a.device, dev);
+    return false;
+  }
+  return true;
+}
+
 }  // namespace
 
 extern "C" int qkx_reCdotXdagY_noalloc(const double* x_dev, const double* y_dev, size_t n_sites, double* result,
@@ -82,6 +114,17 @@ extern "C" int qkx_reCdotXdagY_noalloc(const double* x_dev, const double* y_dev,
     qkx::set_error("device index %d above %d", dev, NA_MAX_DEVICES - 1);
     return QKX_ERR_INVALID;
   }
+  if (!na_field_ok(x_dev, dev, "x") || !na_field_ok(y_dev, dev, "y")) return QKX_ERR_INVALID;
+  cudaStream_t st = (cudaStream_t)stream;
+  {
+    // the result is read back with a synchronizing copy, which a capturing stream cannot do
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    QKX_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (cs != cudaStreamCaptureStatusNone) {
+      qkx::set_error("invalid argument: the stream is capturing; this call synchronizes and cannot be captured");
+      return QKX_ERR_INVALID;
+    }
+  }
   double* scratch = nullptr;
   {
     // first call on this device: look up the device address of the array
@@ -97,7 +140,6 @@ extern "C" int qkx_reCdotXdagY_noalloc(const double* x_dev, const double* y_dev,
     }
     scratch = g_na_ptr[dev];
   }
-  cudaStream_t st = (cudaStream_t)stream;
   const size_t n = 12 * n_sites;  // complex numbers
   const int nblocks = (int)((n + NA_PER_BLOCK - 1) / NA_PER_BLOCK);
   k_na_partials<<<nblocks, NA_NT, 0, st>>>((const double2*)x_dev, (const double2*)y_dev, n, scratch);

@@ -32,7 +32,7 @@ constexpr int TC_ACHUNK = TC_M * TC_K;    // BF16 per colour per chunk (8 KB)
 constexpr int TC_BPATH = TC_N * TC_K;     // BF16 per path of B (2 KB)
 constexpr uint32_t TC_LBO = 128;          // bytes between K-adjacent core matrices
 constexpr uint32_t TC_SBO = 512;          // bytes between M-adjacent core matrices (4 along K)
-constexpr unsigned TC_SPIN = 1u << 26;    // bounded mbarrier polls
+constexpr unsigned long long TC_WAIT_NS = 100000000ull;  // an mbarrier wait gives up after 100 ms
 
 // byte offset of element (row, k) in a [rows][32] K-major no-swizzle canonical tile
 __device__ __forceinline__ uint32_t tc_off(int row, int k) {
@@ -66,9 +66,19 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
                : "memory");
 }
 
+// device clock in nanoseconds
+__device__ __forceinline__ unsigned long long tc_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// wait for phase `parity` of the barrier; false once TC_WAIT_NS of wall time have
+// passed without it (a try_wait may itself suspend, so the bound is on time, not polls)
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
   const uint32_t a = smem_u32(bar);
-  for (unsigned i = 0; i < TC_SPIN; i++) {
+  const unsigned long long t0 = tc_clock_ns();
+  for (;;) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -78,8 +88,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
+    if (tc_clock_ns() - t0 > TC_WAIT_NS) return false;
   }
-  return false;
 }
 
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }

@@ -47,3 +47,22 @@ def test_noalloc_rejects_sizes_above_its_limit(qkx, oracle):
         assert rc == qkx.ERR_INVALID
         assert "limit" in qkx.lib().qkx_last_error().decode()
         x.close()
+
+
+def test_noalloc_rejects_unaligned_and_host_pointers_before_launch(qkx, oracle):
+    # both cases are turned into QKX_ERR_INVALID on the host, before any kernel runs
+    import numpy as np
+    L = (4, 4, 4, 4)
+    with qkx.Lattice(qkx.LatticeInfo(L=L)) as lat:
+        x = lat.field(oracle.spinor_gaussian(L, 4))
+        out = C.c_double()
+        rc = qkx.lib().qkx_reCdotXdagY_noalloc(x.ptr + 8, x.ptr, 16, C.byref(out), None)
+        assert rc == qkx.ERR_INVALID
+        assert "aligned" in qkx.lib().qkx_last_error().decode()
+        host = np.zeros(12 * 2 * lat.V, dtype=np.float64)
+        rc = qkx.lib().qkx_reCdotXdagY_noalloc(x.ptr, host.ctypes.data_as(C.c_void_p), lat.V, C.byref(out), None)
+        assert rc == qkx.ERR_INVALID
+        assert "device memory" in qkx.lib().qkx_last_error().decode()
+        # the library still works after the rejections
+        assert abs(_noalloc(qkx, x, x, lat.V, None) - lat.norm2(x)) <= TOL * lat.norm2(x)
+        x.close()
