@@ -182,11 +182,10 @@ def run_ours(args):
         solve()
     lat.sync()
 
-    # ---- timed region: inputs resident in HBM
+    # ---- timed region: inputs resident in HBM; each solve is one graph launch (the iteration
+    # loop runs on the device) plus the set-up and final kernels
     barrier()
     torch.cuda.synchronize()
-    lat.profile_reset()
-    lat.profile(True)
     k0 = lat.kernel_launches()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     infos = []
@@ -198,10 +197,20 @@ def run_ours(args):
         torch.cuda.synchronize()
     barrier()
     launches = lat.kernel_launches() - k0
-    hop_n, hop_ms, hop_bytes = lat.profile_read()
-    lat.profile(False)
     ms = D.max_over_ranks(e0.elapsed_time(e1))
     step_s = ms / 1e3 / args.steps
+
+    # ---- the dominant kernel, timed: the same solves with CUDA events recorded around every
+    # sloppy hop on the library's stream (the solver then runs its host-driven loop, one graph
+    # per iteration, because event records cannot sit inside the device loop's conditional
+    # nodes; the kernels and their inputs are the same)
+    lat.profile_reset()
+    lat.profile(True)
+    for _ in range(max(1, min(args.steps, 3))):
+        solve()
+    lat.sync()
+    hop_n, hop_ms, hop_bytes = lat.profile_read()
+    lat.profile(False)
 
     # ---- end to end through the host-buffer C ABI
     Uh = Q.pinned_array((V, 4, 3, 3, 2))
@@ -281,7 +290,8 @@ def run_ours(args):
                   "double": "f64"}[args.precision],
         "data": "synthetic (seeded exp(i eps H) links, point sources)",
         "config": {"workload": WORKLOAD, "lattice": "x".join(map(str, L)), "sources_per_gpu": NSRC,
-                   "solver": "even-odd CG, all sources in one batch, CUDA-graph iterations",
+                   "solver": ("even-odd CG, all sources in one batch; the iteration loop is one CUDA graph "
+                              "launch (conditional WHILE nodes, decisions on the device)"),
                    "storage": {"half": "fp16 spinors", "single": "fp32 spinors",
                                "double": "fp64 spinors"}[args.precision] + " + " + hop_links(args.precision, tile),
                    "accumulate": "fp32 inner, fp64 reliable updates / solution / residual checks",
@@ -308,6 +318,7 @@ def run_ours(args):
             "frac": (achieved / peak) if achieved else None,
             "traffic": traffic,
             "launches": hop_n,
+            "timed": "CUDA events around each sloppy hop in profiled solves of the same workload",
             "avg_launch_ms": avg_launch_ms,
             "algorithmic_bytes_per_launch": bytes_per_launch,
         },

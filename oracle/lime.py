@@ -29,9 +29,14 @@ def write_record(f, rtype: str, data: bytes, mb: bool = False, me: bool = False)
 
 
 def ildg_xml(L, precision=64) -> bytes:
-    return ("<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat>\n  <version> 1.0 </version>\n"
-            f"  <field> su3gauge </field>\n  <precision> {precision} </precision>\n  <lx> {L[0]} </lx>\n"
-            f"  <ly> {L[1]} </ly>\n  <lz> {L[2]} </lz>\n  <lt> {L[3]} </lt>\n</ildgFormat>").encode()
+    """The ildg-format text of lib/write_conf_lime.cpp:84, character for character (a
+    writer that is to produce the reference's bytes has to write this exact text)."""
+    return ("<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat xmlns=\"http://www.lqkxTM.org/ildg\"\n"
+            "            xmlns:xsi=\"http://www.w3.org/2001/XMLSchema-instance\"\n"
+            "            xsi:schemaLocation=\"http://www.lqkxTM.org/ildg filefmt.xsd\">\n"
+            f"  <version> 1.0 </version>\n  <field> su3gauge </field>\n  <precision> {precision} </precision>\n"
+            f"  <lx> {L[0]} </lx>\n  <ly> {L[1]} </ly>\n  <lz> {L[2]} </lz>\n  <lt> {L[3]} </lt>\n</ildgFormat>"
+            ).encode()
 
 
 def write_gauge(path, U: np.ndarray, L, precision=64, message=b"test configuration", extra=()) -> None:

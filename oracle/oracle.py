@@ -128,6 +128,8 @@ def ref():
         _ref.ref_ape_smear.argtypes = [_ip, _dp, _dp, C.c_int, C.c_double]
         _ref.ref_gaussian_smear.argtypes = [_ip, _dp, _dp, _dp, C.c_int, C.c_double]
         _ref.ref_absorb_vector.argtypes = [_ip, _dp, C.c_int, C.c_int, _dp]
+        _ref.ref_read_gauge_lime.argtypes = [C.c_char_p, _ip, _dp]
+        _ref.ref_write_gauge_lime.argtypes = [C.c_char_p, _ip, _dp, C.c_char_p]
         _ref.ref_meson_2pt.argtypes = [_ip, _dp, C.c_int, C.c_int, _ip, _dp]
         _ref.ref_baryon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
         _ref.ref_propagator.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
@@ -263,6 +265,24 @@ def ref_cg(L, U, b, kappa, mu, twistSign=1, tol=1e-10, maxIter=1000, x0=None):
     ref().ref_cg(_L(L), kappa, mu, twistSign, tol, maxIter, _ptr(U),
                  _ptr(np.ascontiguousarray(b)), _ptr(x))
     return x
+
+
+def ref_read_gauge_lime(path, L) -> np.ndarray:
+    """qkxTM_MPI_getGaugeLime (lib/read_conf_lime.cpp:111-245), the reference compiled with
+    the LIME and MPI-IO stand-ins of oracle/ref: the file's links as Gauge::M."""
+    U = np.zeros((volume(L), 4, 3, 3, 2))
+    rc = ref().ref_read_gauge_lime(os.fsencode(str(path)), _L(L), _ptr(U))
+    if rc != 0:
+        raise RuntimeError(f"reference LIME reader returned {rc}")
+    return U
+
+
+def ref_write_gauge_lime(path, L, U: np.ndarray, message: bytes) -> None:
+    """qkxTM_writeGaugeLime (lib/write_conf_lime.cpp:49-199): U as an ILDG file."""
+    U = np.ascontiguousarray(U, dtype=np.float64)
+    rc = ref().ref_write_gauge_lime(os.fsencode(str(path)), _L(L), _ptr(U), message)
+    if rc != 0:
+        raise RuntimeError(f"reference LIME writer returned {rc}")
 
 
 def rel_err(a, b) -> float:

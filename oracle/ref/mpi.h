@@ -1,7 +1,8 @@
 /*
  * mpi.h -- single-rank MPI stand-in used ONLY to compile the reference's own
  * hot-path sources (lattice_util.cpp, solvers.cpp, blas_qkxTM.cpp, util.cpp,
- * blas.cpp) into the test oracle under oracle/_ref/.  Test infrastructure.
+ * blas.cpp, contractions.cpp, read_conf_lime.cpp, write_conf_lime.cpp) into the
+ * test oracle under oracle/_ref/.  Test infrastructure.
  *
  * With one rank and P = (1,1,1,1) the reference never exchanges halos
  * (every communicate* call is guarded by lL < L), so point-to-point calls are
@@ -73,5 +74,57 @@ static inline int MPI_Group_incl(MPI_Group, int, const int*, MPI_Group* g) { *g 
 static inline int MPI_Group_rank(MPI_Group, int* r) { *r = 0; return 0; }
 static inline int MPI_Group_size(MPI_Group, int* n) { *n = 1; return 0; }
 static inline int MPI_Comm_create(MPI_Comm, MPI_Group, MPI_Comm* c) { *c = 0; return 0; }
+
+/* MPI-IO for one rank (lib/read_conf_lime.cpp, lib/write_conf_lime.cpp): the subarray a rank
+ * owns is the whole array, so a view is a byte offset and an element size, and a collective
+ * read or write is one contiguous stdio transfer at that offset. */
+#include <stdio.h>
+typedef long long MPI_Offset;
+typedef int MPI_Info;
+typedef struct qkx_stub_file {
+  FILE* fp;
+  MPI_Offset disp;
+  size_t esize;
+} * MPI_File;
+#define MPI_INFO_NULL 0
+#define MPI_MODE_RDONLY 2
+#define MPI_MODE_WRONLY 4
+#define MPI_ORDER_C 56
+
+static inline int MPI_Type_create_subarray(int nd, const int* sizes, const int* sub, const int* starts, int,
+                                           MPI_Datatype old, MPI_Datatype* out) {
+  for (int i = 0; i < nd; i++)
+    if (sub[i] != sizes[i] || starts[i] != 0) return 1; /* one rank owns everything */
+  *out = old;
+  return 0;
+}
+static inline int MPI_File_open(MPI_Comm, const char* name, int amode, MPI_Info, MPI_File* fh) {
+  FILE* fp = fopen(name, amode == MPI_MODE_RDONLY ? "rb" : "r+b");
+  if (!fp) return 1;
+  *fh = new qkx_stub_file{fp, 0, 1};
+  return 0;
+}
+static inline int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype etype, MPI_Datatype, const char*,
+                                    MPI_Info) {
+  fh->disp = disp;
+  fh->esize = qkx_stub_elem_bytes(etype);
+  return 0;
+}
+static inline int MPI_File_read_all(MPI_File fh, void* buf, int count, MPI_Datatype t, MPI_Status*) {
+  const size_t n = (size_t)count * qkx_stub_elem_bytes(t);
+  if (fseeko(fh->fp, (off_t)fh->disp, SEEK_SET) != 0) return 1;
+  return fread(buf, 1, n, fh->fp) == n ? MPI_SUCCESS : 1;
+}
+static inline int MPI_File_write_all(MPI_File fh, const void* buf, int count, MPI_Datatype t, MPI_Status*) {
+  const size_t n = (size_t)count * qkx_stub_elem_bytes(t);
+  if (fseeko(fh->fp, (off_t)fh->disp, SEEK_SET) != 0) return 1;
+  return fwrite(buf, 1, n, fh->fp) == n ? MPI_SUCCESS : 1;
+}
+static inline int MPI_File_close(MPI_File* fh) {
+  const int rc = fclose((*fh)->fp);
+  delete *fh;
+  *fh = 0;
+  return rc == 0 ? MPI_SUCCESS : 1;
+}
 
 #endif

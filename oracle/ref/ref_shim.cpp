@@ -227,6 +227,25 @@ double ref_cg_timed(const int L[4], double kappa, double mu, int twistSign, doub
   return t1 - t0;
 }
 
+/* qkxTM_MPI_getGaugeLime (lib/read_conf_lime.cpp:111-245): the links of an ILDG file into U.
+ * Returns the reference's status (0). */
+int ref_read_gauge_lime(const char* path, const int L[4], double* U) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Gauge u(&li);
+  const int rc = qkxTM_MPI_getGaugeLime(const_cast<char*>(path), u);
+  memcpy(U, &(u.M[0][0][0][0]), sizeof(double) * 72 * volume(L));
+  return rc;
+}
+
+/* qkxTM_writeGaugeLime (lib/write_conf_lime.cpp:49-199): U as an ILDG file with the message as
+ * its xlf-info record.  Returns the reference's status (0). */
+int ref_write_gauge_lime(const char* path, const int L[4], const double* U, const char* message) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Gauge u(&li);
+  memcpy(&(u.M[0][0][0][0]), U, sizeof(double) * 72 * volume(L));
+  return qkxTM_writeGaugeLime(const_cast<char*>(path), u, const_cast<char*>(message));
+}
+
 /* Gauge::calculatePlaquette (lib/lattice_util.cpp:923) of the links as given. */
 double ref_plaquette(const int L[4], const double* U) {
   LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);

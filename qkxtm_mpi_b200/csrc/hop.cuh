@@ -30,6 +30,9 @@ enum Epilogue {
   EPI_XPAY_TWINV = 4,  // out = s (v - i c g5 v), v = a D psi + x (odd-parity reconstruction)
   EPI_XPAY_G5_RES = 5, // res = w - g5 (a D psi + x + i c g5 x), stored in FP32 (hop_c3_kernel only)
   EPI_XPAY_RES = 6,    // res = w - (a D psi + x + i c g5 x), its norm only (hop_c3_kernel only)
+  EPI_XPAY_G5_CGR = 7, // o = g5 (a D psi + x + i c g5 x) is not stored: the CG residual of the batch
+                       // takes it, r -= alpha o, and |r|^2 goes to the norm partials (multi-RHS
+                       // kernels of the mixed solver only; r is racc32, or racc64 for FP64 sloppy)
 };
 
 // extra operands of EPI_XPAY_G5_RES / EPI_XPAY_RES: w, and the FP32 field the residual
@@ -55,6 +58,10 @@ struct HopArgs {
   const double* cvec;  // optional per-RHS factor on c (twisted mass per RHS)
   const double* svec;  // optional per-RHS factor on s
   const int* active;   // optional per-RHS mask; inactive blocks do nothing
+  // EPI_XPAY_G5_CGR only: per-RHS CG step length and the residual batch it updates
+  const double* alpha = nullptr;
+  SpinorF32 racc32{nullptr, nullptr, 0};
+  SpinorF64 racc64{nullptr, nullptr, 0};
 };
 
 template <typename R>

@@ -15,6 +15,8 @@
 // right-hand sides [g*NR, g*NR + NR) of the batch.  (NR, NT) are chosen per
 // lattice and batch by the autotuner (tune_tile in mixed.cu).
 #pragma once
+#include <type_traits>
+
 #include "hop.cuh"
 
 namespace qkx {
@@ -126,13 +128,13 @@ __global__ void __launch_bounds__(NT) hop_mrhs_kernel(HopArgs<SP, GA> A) {
       Spinor<R> o;
       if constexpr (EPI == EPI_PLAIN) {
         o = acc[j];
-      } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5) {
+      } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR) {
         const Spinor<R> v = A.x.shift(r).load(par, cb);
         const Spinor<R> g5v = gamma5<B>(v);
 #pragma unroll
         for (int k = 0; k < 12; k++)
           o.c[k / 3][k % 3] = a * acc[j].c[k / 3][k % 3] + (v.c[k / 3][k % 3] + c * phase<1>(g5v.c[k / 3][k % 3]));
-        if constexpr (EPI == EPI_XPAY_G5) o = gamma5<B>(o);
+        if constexpr (EPI != EPI_XPAY) o = gamma5<B>(o);
       } else if constexpr (EPI == EPI_TWIST_INV) {
         o = twist_inv<B>(acc[j], c, sc);
       } else {  // EPI_XPAY_TWINV
@@ -141,12 +143,30 @@ __global__ void __launch_bounds__(NT) hop_mrhs_kernel(HopArgs<SP, GA> A) {
         for (int k = 0; k < 12; k++) v.c[k / 3][k % 3] = a * acc[j].c[k / 3][k % 3] + v.c[k / 3][k % 3];
         o = twist_inv<B>(v, c, sc);
       }
-      A.out.shift(r).store(par, cb, o);
-      if (A.norm_part) {
+      if constexpr (EPI == EPI_XPAY_G5_CGR) {
+        // the CG residual takes A p directly: r -= alpha A p, |r|^2 in FP64
+        const R al = R(A.alpha[r]);
+        auto rr = [&]() {
+          if constexpr (std::is_same<R, double>::value) return A.racc64.shift(r);
+          else return A.racc32.shift(r);
+        }();
+        Spinor<R> v = rr.load(par, cb);
 #pragma unroll
-        for (int k = 0; k < 12; k++)
-          nrm[j] += double(o.c[k / 3][k % 3].re) * double(o.c[k / 3][k % 3].re) +
-                    double(o.c[k / 3][k % 3].im) * double(o.c[k / 3][k % 3].im);
+        for (int k = 0; k < 12; k++) {
+          Cx<R>& q = v.c[k / 3][k % 3];
+          q.re = q.re - al * o.c[k / 3][k % 3].re;
+          q.im = q.im - al * o.c[k / 3][k % 3].im;
+          nrm[j] += double(q.re) * double(q.re) + double(q.im) * double(q.im);
+        }
+        rr.store(par, cb, v);
+      } else {
+        A.out.shift(r).store(par, cb, o);
+        if (A.norm_part) {
+#pragma unroll
+          for (int k = 0; k < 12; k++)
+            nrm[j] += double(o.c[k / 3][k % 3].re) * double(o.c[k / 3][k % 3].re) +
+                      double(o.c[k / 3][k % 3].im) * double(o.c[k / 3][k % 3].im);
+        }
       }
     }
   }

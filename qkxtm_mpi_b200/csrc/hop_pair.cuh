@@ -247,6 +247,34 @@ __device__ __forceinline__ void load_pair(const uint4* bj, const float* nj, cons
   }
 }
 
+// EPI_XPAY_G5_CGR: the pair's output o = A p is not stored; the CG residual of each
+// stored lane takes it, r -= alpha o (FP32 batch racc32), and |r|^2 is summed in FP64
+__device__ __forceinline__ void pair_cg_update(const HopArgs<SpinorF16, GaugeF16x12>& A, int par, int cb, int rj,
+                                               int rk, bool sj, bool sk, const CP (&o)[4][3], double& nrj,
+                                               double& nrk) {
+#pragma unroll
+  for (int lane = 0; lane < 2; lane++) {
+    const bool on = lane ? sk : sj;
+    if (!on) continue;
+    const int r = lane ? rk : rj;
+    const float al = float(A.alpha[r]);
+    const SpinorF32 rr = A.racc32.shift(r);
+    Spinor<float> v = rr.load(par, cb);
+    double n = 0.0;
+#pragma unroll
+    for (int k = 0; k < 12; k++) {
+      Cx<float>& q = v.c[k / 3][k % 3];
+      const CP& z = o[k / 3][k % 3];
+      q.re = fmaf(-al, lane ? z.re.y : z.re.x, q.re);
+      q.im = fmaf(-al, lane ? z.im.y : z.im.x, q.im);
+      n += double(q.re) * double(q.re) + double(q.im) * double(q.im);
+    }
+    rr.store(par, cb, v);
+    if (lane) nrk = n;
+    else nrj = n;
+  }
+}
+
 template <int NT, int NP, int B, bool DAG, int EPI, int MINB = 1>
 __global__ void __launch_bounds__(NT, MINB) hop_pair_kernel(HopArgs<SpinorF16, GaugeF16x12> A) {
   constexpr int NR = 2 * NP;
@@ -316,8 +344,8 @@ __global__ void __launch_bounds__(NT, MINB) hop_pair_kernel(HopArgs<SpinorF16, G
       if constexpr (EPI == EPI_PLAIN) {
 #pragma unroll
         for (int k = 0; k < 12; k++) o[k / 3][k % 3] = acc[p][k / 3][k % 3];
-      } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5) {
-        // o = a acc + v + i c gamma5 v   (then gamma5 for XPAY_G5)
+      } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR) {
+        // o = a acc + v + i c gamma5 v   (then gamma5 for XPAY_G5 / XPAY_G5_CGR)
         const SpinorF16 xj = A.x.shift(rj), xk = A.x.shift(rk);
         CP v[4][3];
         load_pair((par ? xj.p1 : xj.p0) + cb, (par ? xj.n1 : xj.n0) + cb, (par ? xk.p1 : xk.p0) + cb,
@@ -339,7 +367,7 @@ __global__ void __launch_bounds__(NT, MINB) hop_pair_kernel(HopArgs<SpinorF16, G
 #pragma unroll
         for (int k = 0; k < 12; k++) {
           const int sp = k / 3, a = k % 3;
-          if constexpr (EPI == EPI_XPAY_G5) {
+          if constexpr (EPI != EPI_XPAY) {
             const CP& z = t[g5row<B>(sp)][a];
             if (g5sign<B>(sp) > 0.f) o[sp][a] = z;
             else o[sp][a] = {mul2(bc2(-1.f), z.re), mul2(bc2(-1.f), z.im)};
@@ -375,6 +403,10 @@ __global__ void __launch_bounds__(NT, MINB) hop_pair_kernel(HopArgs<SpinorF16, G
           o[sp][a].re = fma2(cp, z.im, mul2(s2, v[sp][a].re));
           o[sp][a].im = fma2(cn, z.re, mul2(s2, v[sp][a].im));
         }
+      }
+      if constexpr (EPI == EPI_XPAY_G5_CGR) {
+        pair_cg_update(A, par, cb, rj, rk, act[j], act[j + 1], o, nrm[j], nrm[j + 1]);
+        continue;
       }
       const SpinorF16 oj = A.out.shift(rj), ok = A.out.shift(rk);
       store_pair((par ? oj.p1 : oj.p0) + cb, (par ? oj.n1 : oj.n0) + cb, (par ? ok.p1 : ok.p0) + cb,
@@ -497,7 +529,7 @@ __device__ __forceinline__ void pair_epilogue(const HopArgs<SpinorF16, GaugeF16x
   if constexpr (EPI == EPI_PLAIN) {
 #pragma unroll
     for (int k = 0; k < 12; k++) o[k / 3][k % 3] = acc[k / 3][k % 3];
-  } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5) {
+  } else if constexpr (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR) {
     CP v[4][3];
     if constexpr (XPRE) {
 #pragma unroll
@@ -524,7 +556,7 @@ __device__ __forceinline__ void pair_epilogue(const HopArgs<SpinorF16, GaugeF16x
 #pragma unroll
     for (int k = 0; k < 12; k++) {
       const int sp = k / 3, a = k % 3;
-      if constexpr (EPI == EPI_XPAY_G5) {
+      if constexpr (EPI != EPI_XPAY) {
         const CP& z = t[g5row<B>(sp)][a];
         if (g5sign<B>(sp) > 0.f) o[sp][a] = z;
         else o[sp][a] = {mul2(bc2(-1.f), z.re), mul2(bc2(-1.f), z.im)};
@@ -563,6 +595,10 @@ __device__ __forceinline__ void pair_epilogue(const HopArgs<SpinorF16, GaugeF16x
       o[sp][a].re = fma2(cp, z.im, mul2(s2, v[sp][a].re));
       o[sp][a].im = fma2(cn, z.re, mul2(s2, v[sp][a].im));
     }
+  }
+  if constexpr (EPI == EPI_XPAY_G5_CGR) {
+    pair_cg_update(A, par, cb, rj, rk, sj, sk, o, nrj, nrk);
+    return;
   }
   const SpinorF16 oj = A.out.shift(rj), ok = A.out.shift(rk);
   store_pair((par ? oj.p1 : oj.p0) + cb, (par ? oj.n1 : oj.n0) + cb, (par ? ok.p1 : ok.p0) + cb,
@@ -725,7 +761,7 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1) hop_pair_as_kernel(Ho
     if (A.norm_part && tid < 2 && r0 + tid < A.nrhs) A.norm_part[(size_t)(r0 + tid) * A.nblk + blk] = 0.0;
     return;
   }
-  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV);
+  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR || EPI == EPI_XPAY_TWINV);
   const int par = A.out_parity;
   const int cb = blk * NT + tid;
   double nrm[2] = {0.0, 0.0};
@@ -993,7 +1029,7 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
     if (A.norm_part && tid < 2 && r0 + tid < A.nrhs) A.norm_part[(size_t)(r0 + tid) * A.nblk + blk] = 0.0;
     return;
   }
-  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV);
+  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR || EPI == EPI_XPAY_TWINV);
   const int par = A.out_parity;
   const int cb = blk * NT + tid;
   double nrm[2] = {0.0, 0.0};
@@ -1231,7 +1267,7 @@ __global__ void __launch_bounds__(NT, MINB > 0 ? MINB : 1)
     if (A.norm_part && tid < 2 && r0 + tid < A.nrhs) A.norm_part[(size_t)(r0 + tid) * A.nblk + blk] = 0.0;
     return;
   }
-  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV);
+  constexpr bool XOP = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_CGR || EPI == EPI_XPAY_TWINV);
   const int par = A.out_parity;
   const int cb = blk * NT + tid;
   double nrm[2] = {0.0, 0.0};

@@ -253,11 +253,15 @@ int qkx_write_gauge_lime(qkx_ctx* c, const char* path, const double* U_host, con
     return QKX_ERR_CUDA;
   }
 
+  // the ildg-format text of lib/write_conf_lime.cpp:84 character for character, so that the
+  // file is the reference writer's byte for byte
   char xml[1024];
   snprintf(xml, sizeof xml,
-           "<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat>\n  <version> 1.0 </version>\n"
-           "  <field> su3gauge </field>\n  <precision> 64 </precision>\n  <lx> %d </lx>\n  <ly> %d </ly>\n"
-           "  <lz> %d </lz>\n  <lt> %d </lt>\n</ildgFormat>",
+           "<?xml version=\"1.0\" encoding=\"UTF-8\"?>\n<ildgFormat xmlns=\"http://www.lqkxTM.org/ildg\"\n"
+           "            xmlns:xsi=\"http://www.w3.org/2001/XMLSchema-instance\"\n"
+           "            xsi:schemaLocation=\"http://www.lqkxTM.org/ildg filefmt.xsd\">\n"
+           "  <version> 1.0 </version>\n  <field> su3gauge </field>\n  <precision> 64 </precision>\n"
+           "  <lx> %d </lx>\n  <ly> %d </ly>\n  <lz> %d </lz>\n  <lt> %d </lt>\n</ildgFormat>",
            c->p.L[0], c->p.L[1], c->p.L[2], c->p.L[3]);
   const std::string msg = message ? message : "";
   FILE* f = fopen(path, "wb");

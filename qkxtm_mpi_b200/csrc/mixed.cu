@@ -351,6 +351,210 @@ __global__ void k_mx_site(SpinorF64 in, SpinorF64 out, int par, const double* cv
   out.shift(r).store(par, cb, o);
 }
 
+// ---------------------------------------------------------------- device-driven iteration loop
+// The decisions of the reliable-update CG (when to recompute the FP64 residual, which
+// right-hand sides have converged or diverged, where the search direction restarts) are
+// taken on the device by one-block kernels, so that the whole iteration loop is one CUDA
+// graph launch with two conditional WHILE nodes and the host waits once per solve.
+struct MxCtl {
+  double bnorm2[MAX_RHS];  // |b|^2
+  double best[MAX_RHS];    // smallest FP64 true residual^2 so far (|b^|^2 at x = 0)
+  double r2ru[MAX_RHS];    // sloppy r^2 right after the last reliable update
+  double ratio[MAX_RHS];   // |rhat|^2 / |Mh^+ rhat|^2 at the last update
+  double r2rec[MAX_RHS];   // sloppy r^2 of the last iteration
+  double delta2;           // reliable_delta^2
+  double target2;          // (0.9 tol)^2
+  int nrhs, maxIter;
+  int iter, since, n_ru, n_outer, n_restart, diverged;
+  int nan_rhs, nan_iter;   // first right-hand side whose r^2 became NaN or inf, and when (0: none)
+  int unconverged;         // right-hand sides still active when the loop ended
+  unsigned long long t_ru0, ru_ns;  // device clock at the start of the last update; summed update time
+};
+
+__device__ __forceinline__ unsigned long long mx_clock_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// start of the loop (one block of MAX_RHS threads): the per-RHS state from the set-up's norms
+// (|b|^2 in aux, |b^|^2 in aux2, |Mh^+ b^|^2 in r2); the outer loop runs while any RHS is active
+__global__ void __launch_bounds__(MAX_RHS) k_ctl_start(CgScalars* sc, MxCtl* ctl, cudaGraphConditionalHandle h_outer) {
+  const int i = threadIdx.x;
+  bool act = false;
+  if (i < ctl->nrhs) {
+    const double bn = sc->aux[i], rh = sc->aux2[i], r2 = sc->r2[i];
+    ctl->bnorm2[i] = bn;
+    ctl->best[i] = rh;
+    ctl->r2ru[i] = r2;
+    ctl->ratio[i] = r2 > 0 ? rh / r2 : 1.0;
+    ctl->r2rec[i] = 0.0;
+    act = !(bn == 0.0 || r2 == 0.0);
+    sc->active[i] = act ? 1 : 0;
+  }
+  const int any = __syncthreads_or(act);
+  if (i == 0) {
+    ctl->iter = ctl->since = ctl->n_ru = ctl->n_outer = ctl->n_restart = ctl->diverged = 0;
+    ctl->nan_rhs = MAX_RHS;
+    ctl->nan_iter = 0;
+    ctl->unconverged = 0;
+    ctl->ru_ns = 0;
+    cudaGraphSetConditional(h_outer, any ? 1u : 0u);
+  }
+}
+
+// first node of every outer pass: the inner loop runs at least once
+__global__ void k_ctl_inner_begin(cudaGraphConditionalHandle h_inner) { cudaGraphSetConditional(h_inner, 1u); }
+
+// after each inner iteration: the inner loop stops when an RHS asks for a reliable update (its
+// sloppy r^2 fell by delta^2 since the last one, or it looks converged), after 200 iterations
+// without one, at maxIter, or when an r^2 is not finite
+__global__ void __launch_bounds__(MAX_RHS) k_ctl_after_iter(const CgScalars* sc, MxCtl* ctl,
+                                                            cudaGraphConditionalHandle h_inner) {
+  const int i = threadIdx.x;
+  bool act = false, ru = false, bad = false;
+  if (i < ctl->nrhs && sc->active[i]) {
+    act = true;
+    const double r2s = sc->r2[i];
+    if (!(r2s == r2s) || isinf(r2s)) bad = true;
+    ctl->r2rec[i] = r2s;
+    if (r2s < ctl->delta2 * ctl->r2ru[i] || r2s * ctl->ratio[i] <= ctl->target2 * ctl->bnorm2[i]) ru = true;
+  }
+  if (bad) atomicMin(&ctl->nan_rhs, i);
+  const int any_act = __syncthreads_or(act), any_ru = __syncthreads_or(ru), any_bad = __syncthreads_or(bad);
+  if (i == 0) {
+    const int it = ++ctl->iter;
+    const int since = ++ctl->since;
+    if (any_bad && ctl->nan_iter == 0) ctl->nan_iter = it;
+    const bool go = any_act && !any_ru && !any_bad && since < 200 && it < ctl->maxIter;
+    if (!go) ctl->t_ru0 = mx_clock_ns();
+    cudaGraphSetConditional(h_inner, go ? 1u : 0u);
+  }
+}
+
+// after a reliable update (|rhat|^2 in aux, |Mh^+ rhat|^2 in aux2): converged and diverged RHS
+// stop, the others restart their sloppy recursion from the new residual; the outer loop goes
+// on while any RHS is active, below maxIter, with finite residuals
+__global__ void __launch_bounds__(MAX_RHS) k_ctl_after_ru(CgScalars* sc, MxCtl* ctl, cudaGraphConditionalHandle h_outer) {
+  const int i = threadIdx.x;
+  bool act = false, rst = false, div = false;
+  sc->restart[i] = 0;
+  if (i < ctl->nrhs && sc->active[i]) {
+    const double rhat2 = sc->aux[i], r2 = sc->aux2[i];
+    if (rhat2 <= ctl->target2 * ctl->bnorm2[i] || r2 == 0.0) {
+      sc->active[i] = 0;
+    } else if (!(rhat2 <= 1e6 * ctl->best[i])) {  // the true residual grew 1000x above its best
+      sc->active[i] = 0;
+      div = true;
+    } else {
+      ctl->best[i] = fmin(ctl->best[i], rhat2);
+      ctl->ratio[i] = rhat2 / r2;
+      ctl->r2ru[i] = r2;
+      sc->r2[i] = r2;
+      // a residual much larger than the sloppy one it replaces restarts the search direction
+      if (r2 > 4.0 * ctl->r2rec[i]) {
+        sc->restart[i] = 1;
+        rst = true;
+      }
+      act = true;
+    }
+  }
+  const int any_act = __syncthreads_or(act), any_rst = __syncthreads_or(rst), ndiv = __syncthreads_count(div);
+  if (i == 0) {
+    ctl->n_ru++;
+    ctl->n_outer++;
+    ctl->since = 0;
+    ctl->diverged += ndiv;
+    if (any_rst) ctl->n_restart++;
+    ctl->ru_ns += mx_clock_ns() - ctl->t_ru0;
+    const bool go = any_act && ctl->iter < ctl->maxIter && ctl->nan_iter == 0;
+    cudaGraphSetConditional(h_outer, go ? 1u : 0u);
+  }
+}
+
+// after the loop: count the RHS that did not converge; every RHS takes part in the final phase
+__global__ void __launch_bounds__(MAX_RHS) k_ctl_final(CgScalars* sc, MxCtl* ctl) {
+  const int i = threadIdx.x;
+  const bool act = i < ctl->nrhs && sc->active[i];
+  const int n = __syncthreads_count(act);
+  if (i < ctl->nrhs) sc->active[i] = 1;
+  if (i == 0) ctl->unconverged = n;
+}
+
+// Builds the loop graph into `top`: emit(part, h_outer, h_inner) launches the kernels of each
+// part on the context's stream while it is being captured (0: top level before the outer loop,
+// 1: outer body before the inner loop, 2: outer body after it, 3: inner body).  The kernels each
+// part launched come back in *kt, *ko, *ki.  Both handles default to 0 at every launch, so a
+// loop whose condition is never set does not run.
+template <class Emit>
+static int build_loop_graph(qkx_ctx* c, cudaGraph_t top, long long* kt, long long* ko, long long* ki, Emit emit) {
+  bool capturing = false;
+  auto begin = [&](cudaGraph_t g) -> int {
+    QKX_CUDA(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    capturing = true;
+    c->capturing = 1;
+    c->captured = 0;
+    return QKX_OK;
+  };
+  auto end = [&](long long* k) -> int {
+    c->capturing = 0;
+    capturing = false;
+    *k = c->captured;
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(c->st, &g);
+    if (e != cudaSuccess) {
+      set_error("graph capture: %s", cudaGetErrorString(e));
+      return QKX_ERR_CUDA;
+    }
+    return QKX_OK;
+  };
+  // a WHILE node on what the capture has issued so far; later work depends on the node
+  auto add_while = [&](cudaGraphConditionalHandle h, cudaGraph_t* body) -> int {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    QKX_CUDA(cudaStreamGetCaptureInfo(c->st, &cs, nullptr, &g, &deps, &nd));
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node;
+    QKX_CUDA(cudaGraphAddNode(&node, g, deps, nd, &np));
+    *body = np.conditional.phGraph_out[0];
+    QKX_CUDA(cudaStreamUpdateCaptureDependencies(c->st, &node, 1, cudaStreamSetCaptureDependencies));
+    return QKX_OK;
+  };
+  auto run = [&]() -> int {
+    cudaGraphConditionalHandle h_outer = 0, h_inner = 0;
+    cudaGraph_t outer_body = nullptr, inner_body = nullptr;
+    QKX_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top, 0, cudaGraphCondAssignDefault));
+    QKX_TRY(begin(top));
+    QKX_TRY(emit(0, h_outer, h_inner));
+    QKX_TRY(add_while(h_outer, &outer_body));
+    QKX_TRY(end(kt));
+    QKX_CUDA(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, cudaGraphCondAssignDefault));
+    QKX_TRY(begin(outer_body));
+    QKX_TRY(emit(1, h_outer, h_inner));
+    QKX_TRY(add_while(h_inner, &inner_body));
+    QKX_TRY(emit(2, h_outer, h_inner));
+    QKX_TRY(end(ko));
+    QKX_TRY(begin(inner_body));
+    QKX_TRY(emit(3, h_outer, h_inner));
+    QKX_TRY(end(ki));
+    return QKX_OK;
+  };
+  const int rc = run();
+  if (capturing) {  // a failed part: close the capture so the stream is usable again
+    c->capturing = 0;
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(c->st, &g);
+    cudaGetLastError();
+  }
+  return rc;
+}
+
 // ---------------------------------------------------------------- solver state
 struct MixedState {
   int prec = -1;
@@ -362,13 +566,19 @@ struct MixedState {
   double* cvec = nullptr;  // per-RHS 2 kappa mu_r twistSign
   double* svec = nullptr;  // per-RHS 1 / (1 + (2 kappa mu_r)^2)
   double* part = nullptr;  // [R][max(nblk, MX_GRID)]
-  cudaGraphExec_t graph = nullptr;
+  MxCtl* ctl = nullptr;    // decisions of the device-driven loop
+  MxCtl* ctl_h = nullptr;  // page-locked host copy
+  cudaGraphExec_t dgraph = nullptr;  // the device-driven iteration loop
+  int dgraph_R = 0, dgraph_nr = 0, dgraph_nt = 0, dgraph_kind = 0;
+  double dgraph_kappa = 0;
+  long long dgraph_k[3] = {};  // kernels of its top level, outer pass, inner pass
+  cudaGraphExec_t graph = nullptr;  // one iteration (host-driven loop)
   int graph_R = 0;
   int graph_nr = 0, graph_nt = 0, graph_kind = 0;  // hop tile the graph was captured with
   long long graph_kernels = 0;    // kernel nodes in the graph
   double graph_kappa = 0;         // kappa^2 is a kernel argument inside the graph
   std::vector<cudaEvent_t> gev;   // event pairs captured around the hop kernels
-  cudaEvent_t ph[3] = {};         // phase marks: set-up done, reliable update start, its end
+  cudaEvent_t ph[4] = {};         // phase marks: set-up done, reliable update start, its end, final start
 };
 
 void mixed_free(qkx_ctx* c) {
@@ -381,6 +591,9 @@ void mixed_free(qkx_ctx* c) {
   cudaFree(m->svec);
   cudaFree(m->part);
   if (m->graph) cudaGraphExecDestroy(m->graph);
+  if (m->dgraph) cudaGraphExecDestroy(m->dgraph);
+  cudaFree(m->ctl);
+  if (m->ctl_h) cudaFreeHost(m->ctl_h);
   for (auto e : m->gev) cudaEventDestroy(e);
   for (auto e : m->ph)
     if (e) cudaEventDestroy(e);
@@ -419,6 +632,8 @@ static int mixed_alloc(qkx_ctx* c, int R, bool solver) {
     const size_t h64 = sizeof(double2) * 12 * (size_t)Vh * m->R;
     for (double2** f : {&m->bE, &m->bO, &m->x64, &m->g5bh, &m->t64, &m->z64, &m->r64})
       if (rc == QKX_OK && !*f && cudaMalloc(f, h64) != cudaSuccess) rc = QKX_ERR_NOMEM;
+    if (rc == QKX_OK && !m->ctl && cudaMalloc(&m->ctl, sizeof(MxCtl)) != cudaSuccess) rc = QKX_ERR_NOMEM;
+    if (rc == QKX_OK && !m->ctl_h && cudaMallocHost(&m->ctl_h, sizeof(MxCtl)) != cudaSuccess) rc = QKX_ERR_NOMEM;
   }
   if (rc != QKX_OK) {
     mixed_free(c);
@@ -478,6 +693,12 @@ static int launch_mrhs(qkx_ctx* c, int R_, const GA& gauge, const Geom& g, SP in
   A.cvec = m->cvec;
   A.svec = with_s ? m->svec : nullptr;
   A.active = c->sc->active;
+  if constexpr (EPI == EPI_XPAY_G5_CGR) {
+    // the CG residual batch (FP32, or FP64 for FP64 sloppy) and the step lengths
+    A.alpha = c->sc->alpha;
+    if constexpr (std::is_same<R, double>::value) A.racc64 = FieldTraits<SpinorF64>::acc(m->rs, 0, c->Vh);
+    else A.racc32 = FieldTraits<SpinorF32>::acc(m->rs, 0, c->Vh);
+  }
   const int ngrp = (R_ + NR - 1) / NR;
   if (prof_slot >= 0) QKX_CUDA(cudaEventRecordWithFlags(m->gev[2 * prof_slot], c->st, cudaEventRecordExternal));
   constexpr bool f16 = std::is_same<SP, SpinorF16>::value && std::is_same<GA, GaugeF16x12>::value;
@@ -580,12 +801,11 @@ struct Sloppy {
     counted(c);
     QKX_TRY((hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr,
                                                 prof ? 2 : -1)));
-    QKX_TRY((hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, nullptr,
-                                              prof ? 3 : -1)));
+    // A p = g5 (A(-c) y - k^2 D t) goes straight into r -= alpha A p and |r|^2 (never stored)
+    QKX_TRY((hop_tile<SP, GA, R, EPI_XPAY_G5_CGR>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, m->part,
+                                                  prof ? 3 : -1)));
     dim3 gr(MX_GRID, R_);
-    k_mx_update_r<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(Ap, rs, c->sc, m->part);
-    counted(c);
-    k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, MX_GRID, FIN_R2, c->sc);
+    k_mx_finalize<<<R_, 256, 0, c->st>>>(m->part, nblk, FIN_R2, c->sc);
     counted(c);
     k_mx_update_p<SP, AC, R><<<gr, MX_NT, 0, c->st>>>(p, xs, rs, c->sc);
     counted(c);
@@ -594,14 +814,17 @@ struct Sloppy {
   }
 
   // algorithmic bytes of one of the four inner hops, averaged, per RHS in a batch of R_:
-  // per output site the input and output spinors, 8 links shared by the batch in the
-  // tile's link format, and for the two xpay hops one more spinor
+  // per output site the input spinor and 8 links shared by the batch in the tile's link
+  // format, plus the output spinor (hops 1 to 3), the xpay operand (hops 2 and 4) and the
+  // CG residual read and written by the fourth hop's epilogue (FP32, or FP64 for FP64 sloppy)
   static double hop_bytes_per_rhs(qkx_ctx* c, int R_, const HopTile& tile) {
     const double S = P::S, Vh = c->Vh;
+    const double Sr = std::is_same<AC, SpinorF64>::value ? 192.0 : 96.0;
     double G = P::G;
     if (P::id == QKX_PREC_HALF && tile.kind == 9) G = 72.0;  // 18-real FP32 links
     if (P::id == QKX_PREC_HALF && (tile.kind == 10 || tile.kind == 11)) G = 36.0;  // 18-real FP16 links
-    return Vh * ((2 * S + 8 * G / R_) + (3 * S + 8 * G / R_)) / 2.0;
+    const double hops = (2 * S) + (3 * S) + (2 * S) + (2 * S + 2 * Sr);
+    return Vh * (hops / 4.0 + 8 * G / R_);
   }
 };
 
@@ -834,116 +1057,22 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     counted(c);
   }
   QKX_CUDA(cudaGetLastError());
-  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));
-  QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
-  QKX_CUDA(cudaStreamSynchronize(c->st));
-  float ms_setup = 0, ms_ru = 0, ms_seg = 0;
-  QKX_CUDA(cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]));
-  bool ru_pending = false;  // a reliable update's end mark not yet read
+  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));  // set-up done
 
-  // r2rec: the sloppy r^2 when a reliable update was asked for; best: the smallest FP64
-  // true residual ||rhat||^2 seen so far (||b^||^2 at x = 0)
-  std::vector<double> bnorm2(nrhs), r2ru(nrhs), ratio(nrhs, 1.0), r2rec(nrhs, 0.0), best(nrhs);
-  std::vector<int> active(nrhs, 1);
-  int diverged = 0;
-  for (int i = 0; i < nrhs; i++) {
-    bnorm2[i] = sh->aux[i];
-    best[i] = sh->aux2[i];
-    r2ru[i] = sh->r2[i];
-    ratio[i] = sh->r2[i] > 0 ? sh->aux2[i] / sh->r2[i] : 1.0;  // ||rhat||^2 / ||Mh^+ rhat||^2 at x = 0
-    if (bnorm2[i] == 0.0 || sh->r2[i] == 0.0) active[i] = 0;
-    sh->active[i] = active[i];
-  }
-  QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
-
-  // --- graph of one inner iteration
   const bool prof = c->prof != 0;
-  if (prof && m->gev.size() < 8) {
-    for (int e = (int)m->gev.size(); e < 8; e++) {
-      cudaEvent_t ev;
-      QKX_CUDA(cudaEventCreate(&ev));
-      m->gev.push_back(ev);
-    }
-  }
   const bool graphs = sp->use_graphs != 0;
-  if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || m->graph_nr != tile.nr ||
-                   m->graph_nt != tile.nt || m->graph_kind != tile.kind || !graphs || prof)) {
-    cudaGraphExecDestroy(m->graph);
-    m->graph = nullptr;
-  }
-  if (graphs && !m->graph) {
-    cudaGraph_t gr;
-    QKX_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
-    c->capturing = 1;
-    c->captured = 0;
-    int rc = SL::iteration(c, nrhs, prof, tile);
-    c->capturing = 0;
-    m->graph_kernels = c->captured;
-    cudaError_t e = cudaStreamEndCapture(c->st, &gr);
-    if (rc != QKX_OK) return rc;
-    if (e != cudaSuccess) {
-      set_error("graph capture: %s", cudaGetErrorString(e));
-      return QKX_ERR_CUDA;
-    }
-    QKX_CUDA(cudaGraphInstantiate(&m->graph, gr, 0));
-    cudaGraphDestroy(gr);
-    m->graph_R = nrhs;
-    m->graph_kappa = c->p.kappa;
-    m->graph_nr = tile.nr;
-    m->graph_nt = tile.nt;
-    m->graph_kind = tile.kind;
-  }
-
-  const int maxIter = sp->maxIter;
+  // the whole iteration loop on the device (one graph launch) unless the hop kernels are being
+  // timed one by one (event records cannot sit inside a conditional graph body) or graphs are off
+  const bool device_loop = graphs && !prof;
+  const int maxIter = std::min(sp->maxIter, 1000000);
   const double target = 0.9 * sp->tol;
-  int iter = 0, n_ru = 0, since = 0, n_restart = 0;
-  while (iter < maxIter) {
-    int nact = 0;
-    for (int i = 0; i < nrhs; i++) nact += active[i];
-    if (!nact) break;
-    if (m->graph) {
-      QKX_CUDA(cudaGraphLaunch(m->graph, c->st));
-      counted(c, (int)m->graph_kernels);
-    } else {
-      QKX_TRY(SL::iteration(c, nrhs, prof, tile));
-    }
-    iter++;
-    since++;
-    QKX_CUDA(cudaMemcpyAsync(sh->r2, c->sc->r2, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, c->st));
-    QKX_CUDA(cudaStreamSynchronize(c->st));
-    if (ru_pending) {
-      QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
-      ms_ru += ms_seg;
-      ru_pending = false;
-    }
-    if (prof) {
-      for (int h = 0; h < 4; h++) {
-        float ms = 0;
-        QKX_CUDA(cudaEventElapsedTime(&ms, m->gev[2 * h], m->gev[2 * h + 1]));
-        c->prof_ms += ms;
-        c->prof_launches++;
-        c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs, tile) * nact;
-      }
-    }
-    // reliable update of every active RHS when one of them asks for it
-    bool ru = since >= 200;
-    for (int i = 0; i < nrhs; i++) {
-      if (!active[i]) continue;
-      const double r2s = sh->r2[i];
-      if (!(r2s == r2s) || isinf(r2s)) {
-        set_error("mixed CG: r2 of right-hand side %d became %g at iteration %d", i, r2s, iter);
-        return QKX_ERR_NAN;
-      }
-      r2rec[i] = r2s;
-      if (r2s < delta * delta * r2ru[i] || r2s * ratio[i] <= target * target * bnorm2[i]) ru = true;
-    }
-    if (!ru) continue;
-    n_ru++;
-    since = 0;
-    QKX_CUDA(cudaEventRecord(m->ph[1], c->st));
-    // x64 += x_s ; z = g5 b^ - g5 Mh x64 = g5 rhat ; r = Mh^+ rhat
+
+  // reliable update of the active RHS: x64 += x_s (x_s = 0); the FP64 true residual
+  // |rhat|^2 -> aux; the residual the sloppy CG restarts from, Mh^+ rhat, with its norm -> aux2
+  auto reliable_update = [&]() -> int {
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
     counted(c);
+    int nb = 0;
     if constexpr (r32) {
       // the second FP64 hop of Mh x64 forms z = g5 b^ - g5 Mh x64 itself: |z|^2 from the FP64
       // values, z stored in FP32 for the FP32 Mh^+ that follows (straight into the sloppy residual)
@@ -955,85 +1084,272 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
                               true));
       k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbz, FIN_AUX, c->sc);
       counted(c);
-      QKX_TRY(normal_residual_from32(c, nrhs, FA::acc(m->rs, 0, Vh), &nb64));
+      QKX_TRY(normal_residual_from32(c, nrhs, FA::acc(m->rs, 0, Vh), &nb));
     } else {
       QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
       k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
       counted(c);
       k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
       counted(c);
-      QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb64));
+      QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb));
     }
-    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb, FIN_AUX2, c->sc);
     counted(c);
     QKX_CUDA(cudaGetLastError());
-    QKX_CUDA(cudaMemcpyAsync(sh->aux, c->sc->aux, 2 * sizeof(double) * MAX_RHS, cudaMemcpyDeviceToHost, c->st));
-    QKX_CUDA(cudaStreamSynchronize(c->st));
-    bool any_restart = false;
-    for (int i = 0; i < nrhs; i++) {
-      sh->restart[i] = 0;
-      if (!active[i]) continue;
-      const double rhat2 = sh->aux[i], r2 = sh->aux2[i];
-      if (rhat2 <= target * target * bnorm2[i] || r2 == 0.0) {
-        active[i] = 0;
-        sh->active[i] = 0;
-        continue;
-      }
-      if (!(rhat2 <= 1e6 * best[i])) {  // the true residual grew 1000x above its best: diverged
-        active[i] = 0;
-        sh->active[i] = 0;
-        diverged++;
-        continue;
-      }
-      best[i] = std::min(best[i], rhat2);
-      ratio[i] = rhat2 / r2;
-      r2ru[i] = r2;
-      sh->r2[i] = r2;
-      // The search direction was built from the sloppy residual.  When the residual that
-      // replaces it is much larger, alpha = r^2 / <p, A p> of the next step would be too,
-      // so the direction restarts from the new residual.
-      if (r2 > 4.0 * r2rec[i]) {
-        sh->restart[i] = 1;
-        any_restart = true;
-      }
-    }
-    // restart the sloppy residual from the new one for the RHS that go on
-    QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
-    QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+    return QKX_OK;
+  };
+  // after an update's decisions (active and restart flags set): the sloppy residual of the RHS
+  // that go on, and p = r where the search direction restarts
+  auto restart_kernels = [&](bool any_restart) -> int {
     if constexpr (!r32) {
       k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
       counted(c);
     }
     if (any_restart) {
-      n_restart++;
-      QKX_CUDA(cudaMemcpyAsync(c->sc->restart, sh->restart, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
       k_mx_convert<AC, SP><<<cg2, 256, 0, c->st>>>(FA::acc(m->rs, 0, Vh), FT::acc(m->p, 0, Vh), c->sc->restart);
       counted(c);
     }
     QKX_CUDA(cudaGetLastError());
-    QKX_CUDA(cudaEventRecord(m->ph[2], c->st));
-    ru_pending = true;
-  }
-  if (ru_pending) {
-    QKX_CUDA(cudaEventSynchronize(m->ph[2]));
-    QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
-    ms_ru += ms_seg;
-  }
-  // the final phase starts where the last reliable update or iteration ended
-  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));
-  int rc = QKX_OK;
-  int nact = 0;
-  for (int i = 0; i < nrhs; i++) nact += active[i];
-  if (nact) rc = QKX_ERR_NOT_CONVERGED;
+    return QKX_OK;
+  };
 
-  // --- odd parity and the FP64 true residual of the full system, batched
-  for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
-  QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
-  if (nact)  // fold what the unconverged RHS accumulated since their last update
-    {
-      k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
-      counted(c);
+  float ms_setup = 0, ms_ru = 0, ms_seg = 0;
+  int iter = 0, n_ru = 0, n_restart = 0, diverged = 0;
+  std::vector<int> active(nrhs, 1);
+  std::vector<double> bnorm2(nrhs);  // |b|^2 per RHS
+  MxCtl* hc = m->ctl_h;
+
+  if (device_loop) {
+    // --- the iteration loop as one graph: WHILE (any RHS active) { WHILE (no reliable update
+    // asked for) { iteration }; reliable update; decisions }.  Every decision of the host loop
+    // below is taken by a one-block kernel from the same scalars; both loops are bounded by
+    // maxIter because every pass of the outer one runs at least one inner iteration.
+    memset(hc, 0, sizeof(MxCtl));
+    hc->nrhs = nrhs;
+    hc->maxIter = maxIter;
+    hc->delta2 = delta * delta;
+    hc->target2 = target * target;
+    QKX_CUDA(cudaMemcpyAsync(m->ctl, hc, sizeof(MxCtl), cudaMemcpyHostToDevice, c->st));
+    if (m->dgraph && (m->dgraph_R != nrhs || m->dgraph_kappa != c->p.kappa || m->dgraph_nr != tile.nr ||
+                      m->dgraph_nt != tile.nt || m->dgraph_kind != tile.kind)) {
+      QKX_CUDA(cudaStreamSynchronize(c->st));
+      cudaGraphExecDestroy(m->dgraph);
+      m->dgraph = nullptr;
     }
+    if (!m->dgraph) {
+      cudaGraph_t top = nullptr;
+      QKX_CUDA(cudaGraphCreate(&top, 0));
+      long long kt = 0, ko = 0, ki = 0;
+      int rc = build_loop_graph(c, top, &kt, &ko, &ki, [&](int part, cudaGraphConditionalHandle h_outer,
+                                                           cudaGraphConditionalHandle h_inner) -> int {
+        if (part == 0) {  // top level: per-RHS state from the set-up
+          k_ctl_start<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
+          counted(c);
+          return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+        }
+        if (part == 1) {  // outer body before the inner loop
+          k_ctl_inner_begin<<<1, 1, 0, c->st>>>(h_inner);
+          counted(c);
+          return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+        }
+        if (part == 2) {  // outer body after the inner loop
+          QKX_TRY(reliable_update());
+          k_ctl_after_ru<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
+          counted(c);
+          return restart_kernels(true);
+        }
+        // inner body: one iteration and the decision to go on
+        QKX_TRY(SL::iteration(c, nrhs, false, tile));
+        k_ctl_after_iter<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_inner);
+        counted(c);
+        return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+      });
+      if (rc == QKX_OK) {
+        const cudaError_t e = cudaGraphInstantiate(&m->dgraph, top, 0);
+        if (e != cudaSuccess) {
+          set_error("instantiating the solver graph: %s", cudaGetErrorString(e));
+          rc = QKX_ERR_CUDA;
+          m->dgraph = nullptr;
+        }
+      }
+      cudaGraphDestroy(top);
+      if (rc != QKX_OK) return rc;
+      m->dgraph_R = nrhs;
+      m->dgraph_kappa = c->p.kappa;
+      m->dgraph_nr = tile.nr;
+      m->dgraph_nt = tile.nt;
+      m->dgraph_kind = tile.kind;
+      m->dgraph_k[0] = kt;
+      m->dgraph_k[1] = ko;
+      m->dgraph_k[2] = ki;
+    }
+    QKX_CUDA(cudaGraphLaunch(m->dgraph, c->st));
+  } else {
+    // --- host-driven loop: the host reads r^2 after every iteration and takes the decisions
+    QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
+    QKX_CUDA(cudaStreamSynchronize(c->st));
+    bool ru_pending = false;  // a reliable update's end mark not yet read
+
+    // r2rec: the sloppy r^2 when a reliable update was asked for; best: the smallest FP64
+    // true residual ||rhat||^2 seen so far (||b^||^2 at x = 0)
+    std::vector<double> r2ru(nrhs), ratio(nrhs, 1.0), r2rec(nrhs, 0.0), best(nrhs);
+    for (int i = 0; i < nrhs; i++) {
+      bnorm2[i] = sh->aux[i];
+      best[i] = sh->aux2[i];
+      r2ru[i] = sh->r2[i];
+      ratio[i] = sh->r2[i] > 0 ? sh->aux2[i] / sh->r2[i] : 1.0;  // ||rhat||^2 / ||Mh^+ rhat||^2 at x = 0
+      if (bnorm2[i] == 0.0 || sh->r2[i] == 0.0) active[i] = 0;
+      sh->active[i] = active[i];
+    }
+    QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+
+    // --- graph of one inner iteration
+    if (prof && m->gev.size() < 8) {
+      for (int e = (int)m->gev.size(); e < 8; e++) {
+        cudaEvent_t ev;
+        QKX_CUDA(cudaEventCreate(&ev));
+        m->gev.push_back(ev);
+      }
+    }
+    if (m->graph && (m->graph_R != nrhs || m->graph_kappa != c->p.kappa || m->graph_nr != tile.nr ||
+                     m->graph_nt != tile.nt || m->graph_kind != tile.kind || !graphs || prof)) {
+      cudaGraphExecDestroy(m->graph);
+      m->graph = nullptr;
+    }
+    if (graphs && !m->graph) {
+      cudaGraph_t gr;
+      QKX_CUDA(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+      c->capturing = 1;
+      c->captured = 0;
+      int rc = SL::iteration(c, nrhs, prof, tile);
+      c->capturing = 0;
+      m->graph_kernels = c->captured;
+      cudaError_t e = cudaStreamEndCapture(c->st, &gr);
+      if (rc != QKX_OK) return rc;
+      if (e != cudaSuccess) {
+        set_error("graph capture: %s", cudaGetErrorString(e));
+        return QKX_ERR_CUDA;
+      }
+      QKX_CUDA(cudaGraphInstantiate(&m->graph, gr, 0));
+      cudaGraphDestroy(gr);
+      m->graph_R = nrhs;
+      m->graph_kappa = c->p.kappa;
+      m->graph_nr = tile.nr;
+      m->graph_nt = tile.nt;
+      m->graph_kind = tile.kind;
+    }
+
+    int since = 0;
+    while (iter < maxIter) {
+      int nact = 0;
+      for (int i = 0; i < nrhs; i++) nact += active[i];
+      if (!nact) break;
+      if (m->graph) {
+        QKX_CUDA(cudaGraphLaunch(m->graph, c->st));
+        counted(c, (int)m->graph_kernels);
+      } else {
+        QKX_TRY(SL::iteration(c, nrhs, prof, tile));
+      }
+      iter++;
+      since++;
+      QKX_CUDA(cudaMemcpyAsync(sh->r2, c->sc->r2, sizeof(double) * nrhs, cudaMemcpyDeviceToHost, c->st));
+      QKX_CUDA(cudaStreamSynchronize(c->st));
+      if (ru_pending) {
+        QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
+        ms_ru += ms_seg;
+        ru_pending = false;
+      }
+      if (prof) {
+        for (int h = 0; h < 4; h++) {
+          float ms = 0;
+          QKX_CUDA(cudaEventElapsedTime(&ms, m->gev[2 * h], m->gev[2 * h + 1]));
+          c->prof_ms += ms;
+          c->prof_launches++;
+          c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs, tile) * nact;
+        }
+      }
+      // reliable update of every active RHS when one of them asks for it
+      bool ru = since >= 200;
+      for (int i = 0; i < nrhs; i++) {
+        if (!active[i]) continue;
+        const double r2s = sh->r2[i];
+        if (!(r2s == r2s) || isinf(r2s)) {
+          set_error("mixed CG: r2 of right-hand side %d became %g at iteration %d", i, r2s, iter);
+          return QKX_ERR_NAN;
+        }
+        r2rec[i] = r2s;
+        if (r2s < delta * delta * r2ru[i] || r2s * ratio[i] <= target * target * bnorm2[i]) ru = true;
+      }
+      if (!ru) continue;
+      n_ru++;
+      since = 0;
+      QKX_CUDA(cudaEventRecord(m->ph[1], c->st));
+      QKX_TRY(reliable_update());
+      QKX_CUDA(cudaMemcpyAsync(sh->aux, c->sc->aux, 2 * sizeof(double) * MAX_RHS, cudaMemcpyDeviceToHost, c->st));
+      QKX_CUDA(cudaStreamSynchronize(c->st));
+      bool any_restart = false;
+      for (int i = 0; i < nrhs; i++) {
+        sh->restart[i] = 0;
+        if (!active[i]) continue;
+        const double rhat2 = sh->aux[i], r2 = sh->aux2[i];
+        if (rhat2 <= target * target * bnorm2[i] || r2 == 0.0) {
+          active[i] = 0;
+          sh->active[i] = 0;
+          continue;
+        }
+        if (!(rhat2 <= 1e6 * best[i])) {  // the true residual grew 1000x above its best: diverged
+          active[i] = 0;
+          sh->active[i] = 0;
+          diverged++;
+          continue;
+        }
+        best[i] = std::min(best[i], rhat2);
+        ratio[i] = rhat2 / r2;
+        r2ru[i] = r2;
+        sh->r2[i] = r2;
+        // The search direction was built from the sloppy residual.  When the residual that
+        // replaces it is much larger, alpha = r^2 / <p, A p> of the next step would be too,
+        // so the direction restarts from the new residual.
+        if (r2 > 4.0 * r2rec[i]) {
+          sh->restart[i] = 1;
+          any_restart = true;
+        }
+      }
+      // restart the sloppy residual from the new one for the RHS that go on
+      QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+      QKX_CUDA(cudaMemcpyAsync(c->sc->r2, sh->r2, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+      if (any_restart) {
+        n_restart++;
+        QKX_CUDA(cudaMemcpyAsync(c->sc->restart, sh->restart, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+      }
+      QKX_TRY(restart_kernels(any_restart));
+      QKX_CUDA(cudaEventRecord(m->ph[2], c->st));
+      ru_pending = true;
+    }
+    if (ru_pending) {
+      QKX_CUDA(cudaEventSynchronize(m->ph[2]));
+      QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
+      ms_ru += ms_seg;
+    }
+  }
+
+  // --- odd parity and the FP64 true residual of the full system, batched, for every RHS
+  // the final phase starts where the loop ended
+  QKX_CUDA(cudaEventRecord(m->ph[3], c->st));
+  int nact = 0;
+  if (device_loop) {
+    k_ctl_final<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl);
+    counted(c);
+  } else {
+    for (int i = 0; i < nrhs; i++) nact += active[i];
+    for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
+    QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+  }
+  // fold what the unconverged RHS accumulated since their last update (x_s is zero for the others)
+  if (device_loop || nact) {
+    k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+    counted(c);
+  }
   // x_o = A^-1 (b_o + k D_oe x_e) into t64
   QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
                       m->cvec, m->svec, c->sc->active, nullptr, nullptr));
@@ -1051,8 +1367,25 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     QKX_CUDA(cudaMemcpyAsync(x[i] + n12, m->t64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
   }
   QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
+  if (device_loop) QKX_CUDA(cudaMemcpyAsync(hc, m->ctl, sizeof(MxCtl), cudaMemcpyDeviceToHost, c->st));
   QKX_CUDA(cudaEventRecord(c->t1, c->st));
   QKX_CUDA(cudaEventSynchronize(c->t1));
+  QKX_CUDA(cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]));
+  if (device_loop) {
+    iter = hc->iter;
+    n_ru = hc->n_ru;
+    n_restart = hc->n_restart;
+    diverged = hc->diverged;
+    nact = hc->unconverged;
+    ms_ru = float(hc->ru_ns * 1e-6);
+    for (int i = 0; i < nrhs; i++) bnorm2[i] = hc->bnorm2[i];
+    counted(c, (int)(m->dgraph_k[0] + (long long)hc->n_outer * m->dgraph_k[1] + (long long)hc->iter * m->dgraph_k[2]));
+    if (hc->nan_iter > 0) {
+      set_error("mixed CG: r2 of right-hand side %d became non-finite at iteration %d", hc->nan_rhs, hc->nan_iter);
+      return QKX_ERR_NAN;
+    }
+  }
+  int rc = nact ? QKX_ERR_NOT_CONVERGED : QKX_OK;
   double worst = 0.0;
   int it = 0;
   for (int i = 0; i < nrhs; i++) {
@@ -1070,7 +1403,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     info->normal_residual = 0.0;
     float ms = 0, ms_final = 0;
     cudaEventElapsedTime(&ms, c->t0, c->t1);
-    cudaEventElapsedTime(&ms_final, m->ph[0], c->t1);
+    cudaEventElapsedTime(&ms_final, m->ph[3], c->t1);
     info->seconds = ms * 1e-3;
     info->seconds_setup = ms_setup * 1e-3;
     info->seconds_reliable = ms_ru * 1e-3;
@@ -1204,10 +1537,12 @@ int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind,
 
 void mixed_invalidate(qkx_ctx* c) {
   MixedState* m = c->mixed;
-  if (m && m->graph) {
+  if (m && (m->graph || m->dgraph)) {
     cudaStreamSynchronize(c->st);
-    cudaGraphExecDestroy(m->graph);
+    if (m->graph) cudaGraphExecDestroy(m->graph);
+    if (m->dgraph) cudaGraphExecDestroy(m->dgraph);
     m->graph = nullptr;
+    m->dgraph = nullptr;
   }
 }
 

@@ -22,9 +22,15 @@ Fixtures:
 
   ref_contract.npz    Meson::contract / Baryon::contract + fourier(FORWARD) on
                       seeded propagators, lattice 4x2x4x4
+  ref_conf_4x2x2x4.lime
+                      an ILDG configuration written by the reference's own
+                      qkxTM_writeGaugeLime (lib/write_conf_lime.cpp, compiled with
+                      the LIME and MPI-IO stand-ins of oracle/ref), links
+                      apply_bc(gauge_random(L, 0.3, LIME_SEED)), message LIME_MESSAGE
 
     python tests/golden/make_golden.py smear      (only ref_smear.npz)
     python tests/golden/make_golden.py contract   (only ref_contract.npz)
+    python tests/golden/make_golden.py lime       (only ref_conf_4x2x2x4.lime)
 """
 from __future__ import annotations
 
@@ -143,6 +149,18 @@ def make_contract():
     print("ref_contract.npz", os.path.getsize(os.path.join(HERE, "ref_contract.npz")), "bytes")
 
 
+LIME_L = (4, 2, 2, 4)
+LIME_SEED = 77
+LIME_MESSAGE = b"written by the reference's qkxTM_writeGaugeLime"
+
+
+def make_lime():
+    U = O.apply_bc(LIME_L, O.gauge_random(LIME_L, EPS, LIME_SEED), -1)
+    path = os.path.join(HERE, "ref_conf_4x2x2x4.lime")
+    O.ref_write_gauge_lime(path, LIME_L, U, LIME_MESSAGE)
+    print(os.path.basename(path), os.path.getsize(path), "bytes")
+
+
 def main():
     O.build(ref=True)
     if not O.ref_available():
@@ -152,6 +170,9 @@ def main():
         return
     if sys.argv[1:] == ["contract"]:
         make_contract()
+        return
+    if sys.argv[1:] == ["lime"]:
+        make_lime()
         return
 
     # --- small lattice, full outputs
@@ -216,6 +237,7 @@ def main():
         print(f, os.path.getsize(os.path.join(HERE, f)), "bytes")
     make_smear()
     make_contract()
+    make_lime()
 
 
 if __name__ == "__main__":

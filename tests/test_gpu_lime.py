@@ -98,3 +98,26 @@ def test_reader_errors(qkx, oracle, tmp_path):
         # a failed read leaves no gauge field behind
         with pytest.raises(qkx.QkxError):
             lat.tm(oracle.spinor_gaussian(L, 1))
+
+
+def test_reader_and_writer_pinned_to_reference_written_file(qkx, oracle, tmp_path):
+    """tests/golden/ref_conf_4x2x2x4.lime was written by the reference's qkxTM_writeGaugeLime:
+    the library reads exactly its links (as the reference's reader does) and writes the same
+    bytes from them, from host links and from the links a context holds."""
+    import os
+    L = (4, 2, 2, 4)
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_conf_4x2x2x4.lime")
+    U = oracle.apply_bc(L, oracle.gauge_random(L, 0.3, 77), -1)
+    golden = open(path, "rb").read()
+    msg = "written by the reference's qkxTM_writeGaugeLime"
+    with qkx.Lattice(qkx.LatticeInfo(L=L)) as lat:
+        Uh, info = lat.read_gauge_lime(path, qkx.LINKS_AS_GIVEN)
+        assert np.array_equal(Uh, U) and np.array_equal(lat.download_gauge(), U)
+        if oracle.ref_available():
+            assert np.array_equal(Uh, oracle.ref_read_gauge_lime(path, L))
+        p1 = tmp_path / "host.lime"
+        lat.write_gauge_lime(str(p1), U, msg)
+        assert p1.read_bytes() == golden
+        p2 = tmp_path / "ctx.lime"
+        lat.write_gauge_lime(str(p2), None, msg)
+        assert p2.read_bytes() == golden

@@ -91,13 +91,31 @@ def test_multi_mass_batch(qkx, oracle, setup8):
         assert true_res(oracle, L, U, x, b, 0.1615, mu) <= TOL
 
 
-def test_graph_and_eager_agree_bitwise(qkx, oracle, setup8):
+@pytest.mark.parametrize("prec", ["half", "double"])
+def test_device_loop_host_loop_and_eager_agree_bitwise(qkx, oracle, setup8, prec):
+    """The three drivers of the mixed solve take the same decisions from the same scalars and
+    launch the same kernels in the same order: the whole loop as one graph with conditional
+    nodes (the default), one graph per iteration with the decisions on the host (taken while
+    the hop kernels are timed), and eager launches.  Same iterations, reliable updates and
+    restarts, bit-identical solutions, for a batch with a twisted mass per right-hand side."""
     L, U, lat = setup8
-    b = oracle.spinor_gaussian(L, 40)
-    xg, ig = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, use_graphs=1)
-    xe, ie = lat.invert([b], precision=qkx.PREC_HALF, tol=TOL, use_graphs=0)
-    assert ig.iterations == ie.iterations
-    assert np.array_equal(xg[0], xe[0])
+    P = {"half": qkx.PREC_HALF, "double": qkx.PREC_DOUBLE}[prec]
+    bs = [oracle.spinor_gaussian(L, 40 + i) for i in range(3)]
+    runs = []
+    for graphs, prof in ((1, False), (1, True), (0, False)):
+        lat.profile(prof)
+        try:
+            xs, info = lat.invert(bs, precision=P, tol=TOL, use_graphs=graphs)
+        finally:
+            lat.profile(False)
+        runs.append((xs, info))
+    (xd, idv), (xh, ih), (xe, ie) = runs
+    for i in (ih, ie):
+        assert (i.iterations, i.reliable_updates, i.restarts) == (idv.iterations, idv.reliable_updates, idv.restarts)
+    for k in range(len(bs)):
+        assert np.array_equal(xd[k], xh[k]) and np.array_equal(xd[k], xe[k])
+    assert idv.converged == 1 and idv.true_residual <= TOL
+    assert idv.seconds_reliable > 0 and idv.seconds_setup > 0 and idv.seconds_final > 0
 
 
 def test_twist_sign_and_periodic_links(qkx, oracle):
