@@ -386,6 +386,7 @@ class Propagator {
     check(qkx_propagator_absorb(detail::plain_ctx(info_), phi.data(), nu, c2, data()));
   }
   double* data() { return reinterpret_cast<double*>(storage_.data()); }
+  const LatticeInfo& info() const { return info_; }
 
  private:
   LatticeInfo info_;
@@ -452,6 +453,57 @@ inline void contractBaryons(Propagator* prop1, Propagator* prop2, char* twop_fil
                            mom[3 * im + 1], mom[3 * im + 2], g, gp, v[0], v[1]);
             }
     }
+  std::fclose(f);
+}
+
+// contractBaryonsDec (lib/contractions.cpp:916-936): DELTA_ISO1 and DELTA_ISO1O2 for (prop1, prop2)
+// then (prop2, prop1), in Baryon_Dec::dumpData's text format (:869)
+inline void contractBaryonsDec(Propagator* prop1, Propagator* prop2, char* twop_filename, LatticeInfo* latInfo) {
+  qkx_ctx* c = detail::plain_ctx(*latInfo);
+  const int nmom = qkx_momenta(latInfo->Q_sq, nullptr, 0);
+  std::vector<int> mom((size_t)3 * nmom);
+  qkx_momenta(latInfo->Q_sq, mom.data(), nmom);
+  const int Lt = latInfo->L[3];
+  std::vector<double> F((size_t)Lt * nmom * 48 * 2);
+  FILE* f = std::fopen(twop_filename, "w");
+  if (!f) throw Error(QKX_ERR_INVALID, "qkx_b200: cannot open the decuplet output file");
+  Propagator* pairs[2][2] = {{prop1, prop2}, {prop2, prop1}};
+  for (auto& pr : pairs)
+    for (int op = 0; op < 2; op++) {
+      check(qkx_delta_2pt(c, pr[0]->data(), pr[1]->data(), op, latInfo->Q_sq, latInfo->x_src, F.data()));
+      for (int t = 0; t < Lt; t++)
+        for (int im = 0; im < nmom; im++)
+          for (int i = 0; i < 3; i++)
+            for (int g = 0; g < 4; g++)
+              for (int gp = 0; gp < 4; gp++) {
+                const double* v = &F[(((((size_t)t * nmom + im) * 3 + i) * 4 + g) * 4 + gp) * 2];
+                std::fprintf(f, "%d \t %d \t %+d %+d %+d \t %d \t %d %d \t %+e %+e\n", op, t, mom[3 * im],
+                             mom[3 * im + 1], mom[3 * im + 2], i, g, gp, v[0], v[1]);
+              }
+    }
+  std::fclose(f);
+}
+
+// contractNucleon (lib/lattice_util.cpp:3374): the nucleon correlator of (prop1, prop2), per time
+// slice in that function's text format
+inline void contractNucleon(Propagator& prop1, Propagator& prop2, char* output, int Q_sq, int x_src[4]) {
+  qkx_ctx* c = detail::plain_ctx(prop1.info());
+  const int nmom = qkx_momenta(Q_sq, nullptr, 0);
+  std::vector<int> mom((size_t)3 * nmom);
+  qkx_momenta(Q_sq, mom.data(), nmom);
+  const int Lt = prop1.info().L[3];
+  std::vector<double> F((size_t)Lt * nmom * 16 * 2);
+  check(qkx_nucleon_2pt(c, prop1.data(), prop2.data(), Q_sq, x_src, F.data()));
+  FILE* f = std::fopen(output, "w");
+  if (!f) throw Error(QKX_ERR_INVALID, "qkx_b200: cannot open the nucleon output file");
+  for (int t = 0; t < Lt; t++)
+    for (int im = 0; im < nmom; im++)
+      for (int g = 0; g < 4; g++)
+        for (int g1 = 0; g1 < 4; g1++) {
+          const double* v = &F[((((size_t)t * nmom + im) * 4 + g) * 4 + g1) * 2];
+          std::fprintf(f, "%d   %+d %+d %+d   %d %d  \t %+e %+e\n", t, mom[3 * im], mom[3 * im + 1], mom[3 * im + 2],
+                       g, g1, v[0], v[1]);
+        }
   std::fclose(f);
 }
 

@@ -389,6 +389,22 @@ QKX_API int qkx_baryon_2pt(qkx_ctx* ctx, const double* prop1_host, const double*
                            const int x_src[4], double* corr);
 QKX_API int qkx_baryon_2pt_dev(qkx_ctx* ctx, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
                                const int x_src[4], double* corr);
+#define QKX_DELTA_ISO1 0    /* BARYON_DEC_OPERATOR order */
+#define QKX_DELTA_ISO1O2 1
+/* Baryon_Dec::contract(prop1, prop2, op) + Baryon_Dec::fourier(FORWARD)
+ * (lib/contractions.cpp:768-866, :703-741): the decuplet with the three spatial
+ * C gamma_i; corr[t][imom][i][gamma][gamma'] complex (Baryon_Dec::F). */
+QKX_API int qkx_delta_2pt(qkx_ctx* ctx, const double* prop1_host, const double* prop2_host, int op, int Q_sq,
+                          const int x_src[4], double* corr);
+QKX_API int qkx_delta_2pt_dev(qkx_ctx* ctx, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
+                              const int x_src[4], double* corr);
+/* contractNucleon(prop1, prop2, output, Q_sq, x_src) (lib/lattice_util.cpp:3374):
+ * corr[t][imom][gamma][gamma1] complex, the numbers that function prints per time
+ * slice (the C++ layer's contractNucleon writes them in its text format). */
+QKX_API int qkx_nucleon_2pt(qkx_ctx* ctx, const double* prop1_host, const double* prop2_host, int Q_sq,
+                            const int x_src[4], double* corr);
+QKX_API int qkx_nucleon_2pt_dev(qkx_ctx* ctx, const double* prop1_dev, const double* prop2_dev, int Q_sq,
+                                const int x_src[4], double* corr);
 
 /* ---------------------------------------------------------------- ILDG / LIME configurations
  * A LIME file is a sequence of records, each a 144-byte big-endian header

@@ -1,6 +1,7 @@
-// contract.cu -- meson and nucleon two-point functions from propagators
-// (lib/contractions.cpp: Meson::contract :251, Baryon::contract :494, their
-// fourier(FORWARD) :121 / :356 and createMomenta :37) on one B200.
+// contract.cu -- meson, nucleon and decuplet two-point functions from propagators
+// (lib/contractions.cpp: Meson::contract :251, Baryon::contract :494,
+// Baryon_Dec::contract :768, their fourier(FORWARD) :121 / :356 / :703 and
+// createMomenta :37; contractNucleon, lib/lattice_util.cpp:3374) on one B200.
 //
 // A propagator is [V][4][4][3][3] complex in the host layout (Propagator::M).
 // Per site the contraction needs the whole site block (2304 bytes per
@@ -9,6 +10,7 @@
 //   mesons   one thread per (site, operator)
 //   nucleons one thread per (site, gamma, gamma'), each walking the tabulated
 //            spin terms of its (gamma, gamma') and the 36 colour permutations.
+//   decuplet one thread per (site, i, gamma, gamma'), i the spatial C gamma_i.
 // The terms are tabulated on the host in the reference's order (same
 // threshold |value|^2 > 1e-3) from the gamma and charge-conjugation matrices
 // of lib/lattice_util.cpp:255-305.  The Fourier transform is one block per
@@ -166,11 +168,12 @@ __device__ __forceinline__ double2 cm(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 
-// stage CT_SITES site blocks (144 complex each) of a propagator into shared
+// stage NS site blocks (144 complex each) of a propagator into shared
 // memory, site s at sp + s * CT_STRIDE
+template <int NS = CT_SITES>
 __device__ __forceinline__ void stage(double2* sp, const double2* __restrict__ prop, size_t s0, size_t V) {
   const size_t base = s0 * 144;
-  const int total = CT_SITES * 144;
+  const int total = NS * 144;
   for (int i = threadIdx.x; i < total; i += blockDim.x) {
     const size_t site = s0 + i / 144;
     sp[(i / 144) * CT_STRIDE + i % 144] = site < V ? __ldg(prop + base + i) : make_double2(0.0, 0.0);
@@ -254,6 +257,100 @@ __global__ void __launch_bounds__(CT_SITES * 16) k_baryon_sites(const double2* _
         const double2 t = cm(cm(fv, E[b * 3 + b1]), make_double2(x1.x - x2.x, x1.y - x2.y));
         m.x += sign * t.x;
         m.y += sign * t.y;
+      }
+    }
+  }
+  C[(size_t)k * V + site] = m;
+}
+
+// ---- decuplet (Baryon_Dec): per spatial i, the terms (value; alpha, beta, beta', alpha')
+// of (C gamma_i)[alpha][beta] (C gamma_i)bar[beta'][alpha'] in tabulateIndices_Delta's
+// order (lib/contractions.cpp:743-765)
+constexpr int DELTA_MAX_TERMS = 64;
+struct DeltaTerms {
+  int n[3];
+  double2 val[3][DELTA_MAX_TERMS];
+  char4 ab[3][DELTA_MAX_TERMS];  // alpha, beta, beta', alpha'
+};
+
+int delta_terms(const Gammas& g, DeltaTerms& t) {
+  memset(t.n, 0, sizeof t.n);
+  for (int i = 0; i < 3; i++)
+    for (int al = 0; al < 4; al++)
+      for (int be = 0; be < 4; be++)
+        for (int bp = 0; bp < 4; bp++)
+          for (int ap = 0; ap < 4; ap++) {
+            const zc v = g.CG[i][al][be] * g.CGbar[i][bp][ap];
+            if (!keep(v)) continue;
+            if (t.n[i] >= DELTA_MAX_TERMS) return QKX_ERR_INVALID;
+            t.val[i][t.n[i]] = make_double2(v.real(), v.imag());
+            t.ab[i][t.n[i]] = make_char4(al, be, bp, ap);
+            t.n[i]++;
+          }
+  return QKX_OK;
+}
+
+constexpr int DT_SITES = 8;  // sites per block of the decuplet kernel (48 threads a site)
+
+// C[i*16 + gamma*4 + gamma'][site] of Baryon_Dec::contract (lib/contractions.cpp:768-866):
+// one thread per (site, i, gamma, gamma'); op 0 DELTA_ISO1 (three quarks of p1),
+// 1 DELTA_ISO1O2 (p2 for the odd quark, the reference's weights 1/3 x {4, 2, 1}).
+// Each term reads its colour entries from the staged site blocks.
+__global__ void __launch_bounds__(DT_SITES * 48) k_delta_sites(const double2* __restrict__ p1,
+                                                               const double2* __restrict__ p2, size_t V, int op,
+                                                               const DeltaTerms* __restrict__ T,
+                                                               double2* __restrict__ C) {
+  extern __shared__ double2 sb[];
+  double2* s1 = sb;
+  double2* s2 = sb + DT_SITES * CT_STRIDE;
+  const size_t s0 = (size_t)blockIdx.x * DT_SITES;
+  stage<DT_SITES>(s1, p1, s0, V);
+  stage<DT_SITES>(s2, p2, s0, V);
+  __syncthreads();
+  const int ls = threadIdx.x % DT_SITES, k = threadIdx.x / DT_SITES;  // k = i*16 + gamma*4 + gamma'
+  const size_t site = s0 + ls;
+  if (site >= V) return;
+  const int i = k >> 4, g = (k >> 2) & 3, gp = k & 3;
+  const double2* q1 = s1 + ls * CT_STRIDE;
+  const double2* q2 = s2 + ls * CT_STRIDE;
+  // entry [s1][s2][c1][c2] of propagator q
+  auto at = [](const double2* q, int sa, int sb_, int ca, int cb) { return q[sa * 36 + sb_ * 9 + ca * 3 + cb]; };
+  double2 m = make_double2(0.0, 0.0);
+  const int n = T->n[i];
+  for (int idx = 0; idx < n; idx++) {
+    const double2 val = T->val[i][idx];
+    const char4 ab = T->ab[i][idx];
+    const int al = ab.x, be = ab.y, bp = ab.z, ap = ab.w;
+    for (int e1 = 0; e1 < 6; e1++) {
+      const int a = c_eps[e1][0], b = c_eps[e1][1], c = c_eps[e1][2];
+      for (int e2 = 0; e2 < 6; e2++) {
+        const int a1 = c_eps[e2][0], b1 = c_eps[e2][1], c1 = c_eps[e2][2];
+        const double f = (double)(c_sgn[e1] * c_sgn[e2]);
+        double2 t;
+        if (op == 0) {
+          const double2 t1 = cm(cm(at(q1, al, gp, a, c1), at(q1, be, bp, b, b1)), at(q1, g, ap, c, a1));
+          const double2 t2 = cm(cm(at(q1, al, bp, a, b1), at(q1, be, gp, b, c1)), at(q1, g, ap, c, a1));
+          const double2 t3 = cm(cm(at(q1, al, gp, a, c1), at(q1, be, ap, b, a1)), at(q1, g, bp, c, b1));
+          const double2 t4 = cm(cm(at(q1, al, ap, a, a1), at(q1, be, gp, b, c1)), at(q1, g, bp, c, b1));
+          const double2 t5 = cm(cm(at(q1, al, bp, a, b1), at(q1, be, ap, b, a1)), at(q1, g, gp, c, c1));
+          const double2 t6 = cm(cm(at(q1, al, ap, a, a1), at(q1, be, bp, b, b1)), at(q1, g, gp, c, c1));
+          t = make_double2(-t1.x + t2.x + t3.x - t4.x - t5.x + t6.x, -t1.y + t2.y + t3.y - t4.y - t5.y + t6.y);
+        } else {
+          const double2 t1 = cm(cm(at(q1, al, gp, a, c1), at(q2, be, bp, b, b1)), at(q1, g, ap, c, a1));
+          const double2 t2 = cm(cm(at(q1, al, bp, a, b1), at(q2, be, gp, b, c1)), at(q1, g, ap, c, a1));
+          const double2 t3 = cm(cm(at(q1, al, gp, a, c1), at(q1, be, ap, b, a1)), at(q2, g, bp, c, b1));
+          const double2 t4 = cm(cm(at(q1, al, ap, a, a1), at(q1, be, gp, b, c1)), at(q2, g, bp, c, b1));
+          const double2 t5 = cm(cm(at(q1, al, ap, a, a1), at(q2, be, gp, b, c1)), at(q1, g, bp, c, b1));
+          const double2 t6 = cm(cm(at(q1, al, bp, a, b1), at(q1, be, ap, b, a1)), at(q2, g, gp, c, c1));
+          const double2 t7 = cm(cm(at(q1, al, ap, a, a1), at(q1, be, bp, b, b1)), at(q2, g, gp, c, c1));
+          const double2 t8 = cm(cm(at(q1, al, ap, a, a1), at(q2, be, bp, b, b1)), at(q1, g, gp, c, c1));
+          const double third = 1.0 / 3.0;
+          t = make_double2(third * (-4 * t1.x + 2 * t2.x + 2 * t3.x - 2 * t4.x - 2 * t5.x - t6.x + t7.x + 4 * t8.x),
+                           third * (-4 * t1.y + 2 * t2.y + 2 * t3.y - 2 * t4.y - 2 * t5.y - t6.y + t7.y + 4 * t8.y));
+        }
+        const double2 v = cm(make_double2(f * val.x, f * val.y), t);
+        m.x += v.x;
+        m.y += v.y;
       }
     }
   }
@@ -420,6 +517,53 @@ int baryon_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op
   return rc;
 }
 
+int delta_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op, int Q_sq, const int x_src[4],
+              double* corr) {
+  if (!c || !p1 || !p2 || !x_src || !corr) return bad("NULL argument");
+  if (op < 0 || op > 1) return bad("decuplet operator id (0 DELTA_ISO1, 1 DELTA_ISO1O2)");
+  if (Q_sq < 0) return bad("Q_sq < 0");
+  QKX_CUDA(cudaSetDevice(c->device));
+  static const Gammas g;
+  DeltaTerms T;
+  if (delta_terms(g, T) != QKX_OK) return bad("internal: too many spin terms");
+  std::vector<int> mv;
+  const int nmom = host_momenta(Q_sq, mv);
+  if (nmom > 1000) return bad("Q_sq gives more than 1000 momenta (MOM_MAX)");
+  PropIn a, b;
+  QKX_TRY(prop_in(c, p1, host, a));
+  QKX_TRY(prop_in(c, p2, host, b));
+  DeltaTerms* dT = nullptr;
+  double2* C = nullptr;
+  QKX_CUDA(cudaMallocAsync((void**)&dT, sizeof(DeltaTerms), c->st));
+  QKX_CUDA(cudaMallocAsync((void**)&C, sizeof(double2) * 48 * c->V, c->st));
+  QKX_CUDA(cudaMemcpyAsync(dT, &T, sizeof(DeltaTerms), cudaMemcpyHostToDevice, c->st));
+  static bool attr = false;
+  const int smem = (int)(sizeof(double2) * 2 * DT_SITES * CT_STRIDE);
+  if (!attr) {
+    QKX_CUDA(cudaFuncSetAttribute(k_delta_sites, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    attr = true;
+  }
+  const unsigned nb = (unsigned)((c->V + DT_SITES - 1) / DT_SITES);
+  k_delta_sites<<<nb, DT_SITES * 48, smem, c->st>>>(a.d, b.d, c->V, op, dT, C);
+  counted(c);
+  QKX_CUDA(cudaGetLastError());
+  // Baryon_Dec::F is [Lt][Nmom][3][4][4]: one transform of 16 components per i, interleaved
+  const size_t per = (size_t)c->p.L[3] * nmom * 16;
+  std::vector<double> tmp(2 * per);
+  int rc = QKX_OK;
+  for (int i = 0; i < 3 && rc == QKX_OK; i++) {
+    rc = fourier_to_host(c, C + (size_t)i * 16 * c->V, 16, Q_sq, x_src, tmp.data(), nullptr);
+    for (size_t tp = 0; rc == QKX_OK && tp < (size_t)c->p.L[3] * nmom; tp++)
+      memcpy(corr + 2 * (tp * 48 + i * 16), tmp.data() + 2 * tp * 16, sizeof(double) * 32);
+  }
+  cudaFreeAsync(dT, c->st);
+  cudaFreeAsync(C, c->st);
+  if (a.owned) cudaFreeAsync(a.owned, c->st);
+  if (b.owned) cudaFreeAsync(b.owned, c->st);
+  cudaStreamSynchronize(c->st);
+  return rc;
+}
+
 }  // namespace
 }  // namespace qkx
 
@@ -449,6 +593,25 @@ int qkx_baryon_2pt(qkx_ctx* c, const double* prop1_host, const double* prop2_hos
 int qkx_baryon_2pt_dev(qkx_ctx* c, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
                        const int x_src[4], double* corr) {
   return baryon_2pt(c, prop1_dev, prop2_dev, false, op, Q_sq, x_src, corr);
+}
+int qkx_delta_2pt(qkx_ctx* c, const double* prop1_host, const double* prop2_host, int op, int Q_sq,
+                  const int x_src[4], double* corr) {
+  return delta_2pt(c, prop1_host, prop2_host, true, op, Q_sq, x_src, corr);
+}
+int qkx_delta_2pt_dev(qkx_ctx* c, const double* prop1_dev, const double* prop2_dev, int op, int Q_sq,
+                      const int x_src[4], double* corr) {
+  return delta_2pt(c, prop1_dev, prop2_dev, false, op, Q_sq, x_src, corr);
+}
+// contractNucleon's spin terms (its explicit C gamma5 table, lib/lattice_util.cpp:3418-3428,
+// times the table's bar) are Baryon::contract NTN's term for term: C gamma5 there is minus
+// the C gamma_5 of the constructor's tables, and the signs cancel in the product
+int qkx_nucleon_2pt(qkx_ctx* c, const double* prop1_host, const double* prop2_host, int Q_sq, const int x_src[4],
+                    double* corr) {
+  return baryon_2pt(c, prop1_host, prop2_host, true, 0, Q_sq, x_src, corr);
+}
+int qkx_nucleon_2pt_dev(qkx_ctx* c, const double* prop1_dev, const double* prop2_dev, int Q_sq,
+                        const int x_src[4], double* corr) {
+  return baryon_2pt(c, prop1_dev, prop2_dev, false, 0, Q_sq, x_src, corr);
 }
 
 }  // extern "C"
