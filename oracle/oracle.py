@@ -99,6 +99,8 @@ def lib():
         L.orc_momenta.argtypes = [C.c_int, _ip, C.c_int]
         L.orc_meson_2pt.argtypes = [_ip, _dp, C.c_int, C.c_int, _ip, _dp]
         L.orc_baryon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
+        L.orc_delta_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
+        L.orc_nucleon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, _ip, _dp]
         L.orc_ptc_nweights.argtypes = [C.c_int, _ip]
         L.orc_ptc_nweights.restype = C.c_long
         L.orc_ptc_forward.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
@@ -131,6 +133,8 @@ def ref():
         _ref.ref_read_gauge_lime.argtypes = [C.c_char_p, _ip, _dp]
         _ref.ref_write_gauge_lime.argtypes = [C.c_char_p, _ip, _dp, C.c_char_p]
         _ref.ref_meson_2pt.argtypes = [_ip, _dp, C.c_int, C.c_int, _ip, _dp]
+        _ref.ref_delta_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
+        _ref.ref_contract_nucleon.argtypes = [_ip, _dp, _dp, C.c_int, _ip, C.c_char_p]
         _ref.ref_baryon_2pt.argtypes = [_ip, _dp, _dp, C.c_int, C.c_int, _ip, _dp]
         _ref.ref_propagator.argtypes = [_ip, C.c_double, C.c_double, C.c_int, C.c_double, C.c_int,
                                         _dp, _dp, C.c_int, C.c_double, C.c_long, _dp]
@@ -411,6 +415,45 @@ def baryon_2pt(L, prop1, prop2, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
     lib().orc_baryon_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), op, Q_sq,
                          _L(x_src), _ptr(out))
     return out
+
+
+DELTAS = ["ISO1", "ISO1O2"]
+
+
+def delta_2pt(L, prop1, prop2, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    """Baryon_Dec::contract + fourier(FORWARD): [Lt, Nmom, 3, 4, 4, 2]."""
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 3, 4, 4, 2))
+    lib().orc_delta_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), op, Q_sq,
+                        _L(x_src), _ptr(out))
+    return out
+
+
+def nucleon_2pt(L, prop1, prop2, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    """contractNucleon (lib/lattice_util.cpp:3374): [Lt, Nmom, 4, 4, 2]."""
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 4, 4, 2))
+    lib().orc_nucleon_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), Q_sq,
+                          _L(x_src), _ptr(out))
+    return out
+
+
+def ref_delta_2pt(L, prop1, prop2, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:
+    n = len(momenta(Q_sq))
+    out = np.zeros((L[3], n, 3, 4, 4, 2))
+    ref().ref_delta_2pt(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), op, Q_sq,
+                        _L(x_src), _ptr(out))
+    return out
+
+
+def ref_contract_nucleon_text(L, prop1, prop2, Q_sq, x_src, path) -> np.ndarray:
+    """contractNucleon of the compiled reference: it writes its correlator as text to
+    `path`; returned as [Lt, Nmom, 4, 4, 2] at the printed precision (%+e, 7 digits)."""
+    ref().ref_contract_nucleon(_L(L), _ptr(np.ascontiguousarray(prop1)), _ptr(np.ascontiguousarray(prop2)), Q_sq,
+                               _L(x_src), os.fsencode(str(path)))
+    rows = [ln.split() for ln in open(path) if ln.strip()]
+    n = len(momenta(Q_sq))
+    return np.array([[float(r[-2]), float(r[-1])] for r in rows]).reshape(L[3], n, 4, 4, 2)
 
 
 def ref_meson_2pt(L, prop, op, Q_sq=0, x_src=(0, 0, 0, 0)) -> np.ndarray:

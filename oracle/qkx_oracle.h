@@ -95,6 +95,13 @@ int orc_momenta(int Q_sq, int* mom, int max);
 int orc_meson_2pt(const int L[4], const double* prop, int op, int Q_sq, const int x_src[4], double* corr);
 int orc_baryon_2pt(const int L[4], const double* prop1, const double* prop2, int op, int Q_sq, const int x_src[4],
                    double* corr);
+/* Baryon_Dec::contract + fourier(FORWARD) (lib/contractions.cpp:703-870): corr is
+ * [Lt][Nmom][3][4][4]; op 0 DELTA_ISO1, 1 DELTA_ISO1O2. */
+int orc_delta_2pt(const int L[4], const double* prop1, const double* prop2, int op, int Q_sq, const int x_src[4],
+                  double* corr);
+/* contractNucleon (lib/lattice_util.cpp:3374): corr is [Lt][Nmom][4][4]. */
+int orc_nucleon_2pt(const int L[4], const double* prop1, const double* prop2, int Q_sq, const int x_src[4],
+                    double* corr);
 
 /* learned preconditioner (qkx_oracle_ptc.c; no reference counterpart): a linear
  * parallel-transport convolution network with nlayers layers of channel widths

@@ -270,3 +270,167 @@ int orc_baryon_2pt(const int L[4], const double* p1d, const double* p2d, int op,
   free(M);
   return nmom;
 }
+
+/* Baryon_Dec::contract(prop1, prop2, op) then Baryon_Dec::fourier(FORWARD)
+ * (lib/contractions.cpp:744-870, :703-741, tabulateIndices_Delta :743-765):
+ * corr[t][imom][i][gamma][gammap], i = 0..2 the spatial C gamma_i;
+ * op 0 = DELTA_ISO1 (three prop1 quarks), 1 = DELTA_ISO1O2 (prop2 as the odd one).
+ * Terms, colour sums and the eight (six) products of each term are accumulated in
+ * the reference's order, so the result is the reference's to the last bit. */
+int orc_delta_2pt(const int L[4], const double* p1d, const double* p2d, int op, int Q_sq, const int x_src[4],
+                  double* corrd) {
+  tables();
+  const cplx* P1 = (const cplx*)p1d;
+  const cplx* P2 = (const cplx*)p2d;
+  cplx* corr = (cplx*)corrd;
+  const long V = orc_volume(L);
+  cplx val[3][16];
+  int ind[3][4][16], cnt[3] = {0, 0, 0};
+  for (int i = 0; i < 3; i++)
+    for (int al = 0; al < 4; al++)
+      for (int be = 0; be < 4; be++)
+        for (int bp = 0; bp < 4; bp++)
+          for (int ap = 0; ap < 4; ap++) {
+            const cplx t = CG[i][al][be] * CG_bar[i][bp][ap];
+            if (norm2c(t) > 1e-3) {
+              val[i][cnt[i]] = t;
+              ind[i][0][cnt[i]] = al, ind[i][1][cnt[i]] = be, ind[i][2][cnt[i]] = bp, ind[i][3][cnt[i]] = ap;
+              cnt[i]++;
+            }
+          }
+  cplx* M = (cplx*)calloc((size_t)V * 48, sizeof(cplx));
+#define P(Q, s1, s2, c1, c2) (Q)[v * 144 + (s1) * 36 + (s2) * 9 + (c1) * 3 + (c2)]
+  for (long v = 0; v < V; v++)
+    for (int i = 0; i < 3; i++)
+      for (int g = 0; g < 4; g++)
+        for (int gp = 0; gp < 4; gp++) {
+          cplx m = 0;
+          for (int idx = 0; idx < cnt[i]; idx++) {
+            const int al = ind[i][0][idx], be = ind[i][1][idx], bp = ind[i][2][idx], ap = ind[i][3][idx];
+            for (int e1 = 0; e1 < 6; e1++) {
+              const int a = EPS[e1][0], b = EPS[e1][1], c = EPS[e1][2];
+              for (int e2 = 0; e2 < 6; e2++) {
+                const int a1 = EPS[e2][0], b1 = EPS[e2][1], c1 = EPS[e2][2];
+                const cplx factor = (double)(SGN_EPS[e1] * SGN_EPS[e2]) * val[i][idx];
+                if (op == 0) {
+                  const cplx t = -P(P1, al, gp, a, c1) * P(P1, be, bp, b, b1) * P(P1, g, ap, c, a1) +
+                                 P(P1, al, bp, a, b1) * P(P1, be, gp, b, c1) * P(P1, g, ap, c, a1) +
+                                 P(P1, al, gp, a, c1) * P(P1, be, ap, b, a1) * P(P1, g, bp, c, b1) -
+                                 P(P1, al, ap, a, a1) * P(P1, be, gp, b, c1) * P(P1, g, bp, c, b1) -
+                                 P(P1, al, bp, a, b1) * P(P1, be, ap, b, a1) * P(P1, g, gp, c, c1) +
+                                 P(P1, al, ap, a, a1) * P(P1, be, bp, b, b1) * P(P1, g, gp, c, c1);
+                  m = m + factor * t;
+                } else {
+                  const cplx t = -4.0 * P(P1, al, gp, a, c1) * P(P2, be, bp, b, b1) * P(P1, g, ap, c, a1) +
+                                 2.0 * P(P1, al, bp, a, b1) * P(P2, be, gp, b, c1) * P(P1, g, ap, c, a1) +
+                                 2.0 * P(P1, al, gp, a, c1) * P(P1, be, ap, b, a1) * P(P2, g, bp, c, b1) -
+                                 2.0 * P(P1, al, ap, a, a1) * P(P1, be, gp, b, c1) * P(P2, g, bp, c, b1) -
+                                 2.0 * P(P1, al, ap, a, a1) * P(P2, be, gp, b, c1) * P(P1, g, bp, c, b1) -
+                                 P(P1, al, bp, a, b1) * P(P1, be, ap, b, a1) * P(P2, g, gp, c, c1) +
+                                 P(P1, al, ap, a, a1) * P(P1, be, bp, b, b1) * P(P2, g, gp, c, c1) +
+                                 4.0 * P(P1, al, ap, a, a1) * P(P2, be, bp, b, b1) * P(P1, g, gp, c, c1);
+                  m = m + factor * (1. / 3.) * t;
+                }
+              }
+            }
+          }
+          M[v * 48 + i * 16 + g * 4 + gp] = m;
+        }
+#undef P
+  int mom[3000];
+  const int nmom = orc_momenta(Q_sq, mom, 1000);
+  const long V3 = (long)L[0] * L[1] * L[2];
+  for (int i = 0; i < 3; i++)
+    for (int t = 0; t < L[3]; t++)
+      for (int im = 0; im < nmom; im++)
+        for (int k = 0; k < 16; k++) {
+          cplx s = 0;
+          for (int z = 0; z < L[2]; z++)
+            for (int y = 0; y < L[1]; y++)
+              for (int x = 0; x < L[0]; x++) {
+                const long v = t * V3 + x + (long)L[0] * (y + (long)L[1] * z);
+                const double th = (((double)mom[3 * im] * (x - x_src[0])) / L[0] +
+                                   ((double)mom[3 * im + 1] * (y - x_src[1])) / L[1] +
+                                   ((double)mom[3 * im + 2] * (z - x_src[2])) / L[2]) * 2 * REF_PI;
+                s = s + M[v * 48 + i * 16 + k] * (cos(th) - _Complex_I * sin(th));
+              }
+          corr[((long)t * nmom + im) * 48 + i * 16 + k] = s;
+        }
+  free(M);
+  return nmom;
+}
+
+/* contractNucleon(prop1, prop2, output, Q_sq, x_src) (lib/lattice_util.cpp:3374-3528):
+ * the nucleon two-point function with the explicit C gamma5 table of :3418-3428, per
+ * time slice the spin block summed in the reference's order (each colour term as
+ * two separate updates) and its Fourier transform; corr[t][imom][gamma][gamma1] are
+ * the numbers that function prints. */
+int orc_nucleon_2pt(const int L[4], const double* p1d, const double* p2d, int Q_sq, const int x_src[4],
+                    double* corrd) {
+  const cplx* P1 = (const cplx*)p1d;
+  const cplx* P2 = (const cplx*)p2d;
+  cplx* corr = (cplx*)corrd;
+  cplx cg5[4][4], cg5b[4][4];
+  memset(cg5, 0, sizeof cg5);
+  memset(cg5b, 0, sizeof cg5b);
+  cg5[0][1] = 1, cg5[1][0] = -1, cg5[2][3] = 1, cg5[3][2] = -1;
+  cg5b[0][1] = -1, cg5b[1][0] = 1, cg5b[2][3] = -1, cg5b[3][2] = 1;
+  cplx val[256];
+  int ind[256][4], cnt = 0;
+  for (int al = 0; al < 4; al++)
+    for (int be = 0; be < 4; be++)
+      for (int b1 = 0; b1 < 4; b1++)
+        for (int a1 = 0; a1 < 4; a1++) {
+          const cplx t = cg5[al][be] * cg5b[b1][a1];
+          if (norm2c(t) > 1e-3) {
+            val[cnt] = t;
+            ind[cnt][0] = al, ind[cnt][1] = be, ind[cnt][2] = b1, ind[cnt][3] = a1;
+            cnt++;
+          }
+        }
+  int mom[3000];
+  const int nmom = orc_momenta(Q_sq, mom, 1000);
+  const long V3 = (long)L[0] * L[1] * L[2];
+  cplx* block = (cplx*)calloc((size_t)V3 * 16, sizeof(cplx));
+#define P(Q, s1, s2, c1, c2) (Q)[v * 144 + (s1) * 36 + (s2) * 9 + (c1) * 3 + (c2)]
+  for (int t = 0; t < L[3]; t++) {
+    memset(block, 0, sizeof(cplx) * V3 * 16);
+    for (long v3 = 0; v3 < V3; v3++) {
+      const long v = t * V3 + v3;
+      for (int g = 0; g < 4; g++)
+        for (int g1 = 0; g1 < 4; g1++) {
+          cplx bl = 0;
+          for (int idx = 0; idx < cnt; idx++) {
+            const int al = ind[idx][0], be = ind[idx][1], bb1 = ind[idx][2], aa1 = ind[idx][3];
+            for (int e1 = 0; e1 < 6; e1++) {
+              const int a = EPS[e1][0], b = EPS[e1][1], c = EPS[e1][2];
+              for (int e2 = 0; e2 < 6; e2++) {
+                const int a1 = EPS[e2][0], b1 = EPS[e2][1], c1 = EPS[e2][2];
+                const cplx factor = (double)(SGN_EPS[e1] * SGN_EPS[e2]) * val[idx];
+                bl = bl + factor * P(P2, be, bb1, b, b1) * P(P1, al, aa1, a, a1) * P(P1, g, g1, c, c1);
+                bl = bl - factor * P(P2, be, bb1, b, b1) * P(P1, al, g1, a, c1) * P(P1, g, aa1, c, a1);
+              }
+            }
+          }
+          block[v3 * 16 + g * 4 + g1] = bl;
+        }
+    }
+    for (int im = 0; im < nmom; im++)
+      for (int k = 0; k < 16; k++) {
+        cplx s = 0;
+        for (int z = 0; z < L[2]; z++)
+          for (int y = 0; y < L[1]; y++)
+            for (int x = 0; x < L[0]; x++) {
+              const long v3 = x + (long)L[0] * (y + (long)L[1] * z);
+              const double th = (((double)mom[3 * im] * (x - x_src[0])) / L[0] +
+                                 ((double)mom[3 * im + 1] * (y - x_src[1])) / L[1] +
+                                 ((double)mom[3 * im + 2] * (z - x_src[2])) / L[2]) * 2 * REF_PI;
+              s = s + block[v3 * 16 + k] * (cos(th) - _Complex_I * sin(th));
+            }
+        corr[((long)t * nmom + im) * 16 + k] = s;
+      }
+  }
+#undef P
+  free(block);
+  return nmom;
+}

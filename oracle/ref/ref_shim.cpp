@@ -389,4 +389,40 @@ int ref_baryon_2pt(const int L[4], const double* prop1, const double* prop2, int
   return nmom;
 }
 
+/* Baryon_Dec::contract(prop1, prop2, op) and fourier(FORWARD) (lib/contractions.cpp:703-870);
+ * corr receives Baryon_Dec::F ([Lt][Nmom][3][4][4] complex).  Returns Nmom. */
+int ref_delta_2pt(const int L[4], const double* prop1, const double* prop2, int op, int Q_sq, const int x_src[4],
+                  double* corr) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  li.Q_sq = Q_sq;
+  for (int i = 0; i < 4; i++) li.x_src[i] = x_src[i];
+  Propagator p1(&li), p2(&li);
+  memcpy(&(p1.M[0][0][0][0][0]), prop1, sizeof(double) * 288 * volume(L));
+  memcpy(&(p2.M[0][0][0][0][0]), prop2, sizeof(double) * 288 * volume(L));
+  char devnull[] = "/dev/null";
+  int nmom;
+  {
+    QuietStdout q;
+    Baryon_Dec d(&li, devnull);
+    d.contract(p1, p2, (BARYON_DEC_OPERATOR)op);
+    d.fourier(FORWARD);
+    nmom = d.Nmom;
+    memcpy(corr, d.F, sizeof(double) * 96 * L[3] * nmom);
+  }
+  return nmom;
+}
+
+/* contractNucleon(prop1, prop2, output, Q_sq, x_src) (lib/lattice_util.cpp:3374): the
+ * reference writes its correlator as text to `output`. */
+void ref_contract_nucleon(const int L[4], const double* prop1, const double* prop2, int Q_sq, const int x_src[4],
+                          const char* output) {
+  LatticeInfo li = make_info(L, 0.1, 0.0, 1, -1, 1e-10, 1000);
+  Propagator p1(&li), p2(&li);
+  memcpy(&(p1.M[0][0][0][0][0]), prop1, sizeof(double) * 288 * volume(L));
+  memcpy(&(p2.M[0][0][0][0][0]), prop2, sizeof(double) * 288 * volume(L));
+  int xs[4] = {x_src[0], x_src[1], x_src[2], x_src[3]};
+  QuietStdout q;
+  contractNucleon(p1, p2, const_cast<char*>(output), Q_sq, xs);
+}
+
 }  // extern "C"

@@ -74,7 +74,8 @@ SYMBOLS = [
     "qkx_propagator_dev", "qkx_ptc_create", "qkx_ptc_destroy", "qkx_ptc_num_weights", "qkx_ptc_get_weights",
     "qkx_ptc_set_weights", "qkx_ptc_apply", "qkx_ptc_loss_grad", "qkx_ptc_train",
     "qkx_read_gauge_lime", "qkx_write_gauge_lime", "qkx_momenta", "qkx_meson_2pt", "qkx_meson_2pt_dev",
-    "qkx_baryon_2pt", "qkx_baryon_2pt_dev", "qkx_invert_batch",
+    "qkx_baryon_2pt", "qkx_baryon_2pt_dev", "qkx_delta_2pt", "qkx_delta_2pt_dev", "qkx_nucleon_2pt",
+    "qkx_nucleon_2pt_dev", "qkx_invert_batch",
 ]
 
 
@@ -232,6 +233,10 @@ def lib() -> C.CDLL:
         L.qkx_meson_2pt_dev.argtypes = L.qkx_meson_2pt.argtypes
         L.qkx_baryon_2pt.argtypes = [_vp, _vp, _vp, C.c_int, C.c_int, C.POINTER(C.c_int), _vp]
         L.qkx_baryon_2pt_dev.argtypes = L.qkx_baryon_2pt.argtypes
+        L.qkx_delta_2pt.argtypes = L.qkx_baryon_2pt.argtypes
+        L.qkx_delta_2pt_dev.argtypes = L.qkx_baryon_2pt.argtypes
+        L.qkx_nucleon_2pt.argtypes = [_vp, _vp, _vp, C.c_int, C.POINTER(C.c_int), _vp]
+        L.qkx_nucleon_2pt_dev.argtypes = L.qkx_nucleon_2pt.argtypes
         _lib = L
     return _lib
 
@@ -577,6 +582,28 @@ class Lattice:
         check(f(self.ctx, p1, p2, op, Q_sq, (C.c_int * 4)(*x_src), out.ctypes.data))
         return out
 
+    def delta_2pt(self, prop1, prop2, op: int, Q_sq: int = 0, x_src=(0, 0, 0, 0), device: bool = False):
+        """Baryon_Dec::contract(prop1, prop2, op) + fourier(FORWARD): [Lt, Nmom, 3, 4, 4, 2]
+        (op 0 DELTA_ISO1, 1 DELTA_ISO1O2)."""
+        nmom = len(momenta(Q_sq))
+        out = np.zeros((self.info.L[3], nmom, 3, 4, 4, 2))
+        f = lib().qkx_delta_2pt_dev if device else lib().qkx_delta_2pt
+        p1 = prop1 if device else _host(prop1).ctypes.data
+        p2 = prop2 if device else _host(prop2).ctypes.data
+        check(f(self.ctx, p1, p2, op, Q_sq, (C.c_int * 4)(*x_src), out.ctypes.data))
+        return out
+
+    def nucleon_2pt(self, prop1, prop2, Q_sq: int = 0, x_src=(0, 0, 0, 0), device: bool = False):
+        """contractNucleon(prop1, prop2, ..., Q_sq, x_src) (lib/lattice_util.cpp:3374): the
+        numbers it prints, as [Lt, Nmom, 4, 4, 2]."""
+        nmom = len(momenta(Q_sq))
+        out = np.zeros((self.info.L[3], nmom, 4, 4, 2))
+        f = lib().qkx_nucleon_2pt_dev if device else lib().qkx_nucleon_2pt
+        p1 = prop1 if device else _host(prop1).ctypes.data
+        p2 = prop2 if device else _host(prop2).ctypes.data
+        check(f(self.ctx, p1, p2, Q_sq, (C.c_int * 4)(*x_src), out.ctypes.data))
+        return out
+
     # ------------------------------------------------------------ profiling
     def profile(self, on: bool) -> None:
         check(lib().qkx_profile_enable(self.ctx, int(on)))
@@ -719,6 +746,7 @@ def invert_batch(jobs, method: int = SOLVER_CG_EO_MIXED, precision: int = PREC_H
 
 MESONS = ["ONE", "G5", "G1", "G2", "G3", "G4", "G5G1", "G5G2", "G5G3", "G5G4"]
 BARYONS = ["NTN", "NTR", "RTN", "RTR"]
+DELTAS = ["ISO1", "ISO1O2"]
 
 
 def momenta(Q_sq: int) -> np.ndarray:

@@ -20,8 +20,9 @@ Fixtures:
                       Vector::Gaussian_smearing and the propagator loop of
                       bin/test_invert_prop.cpp, lattice 4x4x4x8
 
-  ref_contract.npz    Meson::contract / Baryon::contract + fourier(FORWARD) on
-                      seeded propagators, lattice 4x2x4x4
+  ref_contract.npz    Meson::contract / Baryon::contract / Baryon_Dec::contract +
+                      fourier(FORWARD) on seeded propagators, lattice 4x2x4x4, and
+                      the numbers contractNucleon prints for them (its text output)
   ref_conf_4x2x2x4.lime
                       an ILDG configuration written by the reference's own
                       qkxTM_writeGaugeLime (lib/write_conf_lime.cpp, compiled with
@@ -145,6 +146,11 @@ def make_contract():
         d[f"meson:{name}"] = O.ref_meson_2pt(L, p1, op, c["Q_sq"], c["x_src"])
     for op, name in enumerate(O.BARYONS):
         d[f"baryon:{name}"] = O.ref_baryon_2pt(L, p1, p2, op, c["Q_sq"], c["x_src"])
+    for op, name in enumerate(O.DELTAS):
+        d[f"delta:{name}"] = O.ref_delta_2pt(L, p1, p2, op, c["Q_sq"], c["x_src"])
+    import tempfile
+    with tempfile.TemporaryDirectory() as tmp:
+        d["nucleon_text"] = O.ref_contract_nucleon_text(L, p1, p2, c["Q_sq"], c["x_src"], os.path.join(tmp, "n.txt"))
     np.savez_compressed(os.path.join(HERE, "ref_contract.npz"), **d)
     print("ref_contract.npz", os.path.getsize(os.path.join(HERE, "ref_contract.npz")), "bytes")
 

@@ -1,5 +1,6 @@
-"""GPU parity of the two-point contractions (qkx_meson_2pt / qkx_baryon_2pt,
-lib/contractions.cpp Meson/Baryon::contract + fourier) against the oracle and
+"""GPU parity of the two-point contractions (qkx_meson_2pt / qkx_baryon_2pt /
+qkx_delta_2pt / qkx_nucleon_2pt: lib/contractions.cpp Meson/Baryon/Baryon_Dec::contract
++ fourier, contractNucleon of lib/lattice_util.cpp) against the oracle and
 the golden vectors from the reference.  FP64; the GPU sums the Fourier
 transform in a different order and contracts complex products with FMA, so the
 bar is 1e-12 relative to the largest correlator entry."""
@@ -35,6 +36,11 @@ def test_golden(qkx):
             assert _close(m[op], g[f"meson:{name}"]), name
         for op, name in enumerate(qkx.BARYONS):
             assert _close(lat.baryon_2pt(p1, p2, op, Q, xs), g[f"baryon:{name}"]), name
+        for op, name in enumerate(qkx.DELTAS):
+            assert _close(lat.delta_2pt(p1, p2, op, Q, xs), g[f"delta:{name}"]), name
+        n = lat.nucleon_2pt(p1, p2, Q, xs)
+        assert _close(n, g["baryon:NTN"])
+        assert np.abs(n - g["nucleon_text"]).max() <= 1e-6 * np.abs(n).max()
 
 
 @pytest.mark.parametrize("L,Q,xs", [((4, 4, 4, 8), 0, (0, 0, 0, 0)), ((6, 4, 2, 10), 1, (5, 3, 1, 9)),
@@ -48,6 +54,10 @@ def test_vs_oracle(qkx, oracle, L, Q, xs):
             assert _close(m[i], oracle.meson_2pt(L, p1, op, Q, xs)), (L, op)
         for op in (range(4) if L[0] != 8 else (0, 3)):
             assert _close(lat.baryon_2pt(p1, p2, op, Q, xs), oracle.baryon_2pt(L, p1, p2, op, Q, xs)), (L, op)
+        if L[0] != 8:  # the decuplet oracle is slow: 48 components x 576 colour-spin terms a site
+            for op in range(2):
+                assert _close(lat.delta_2pt(p1, p2, op, Q, xs), oracle.delta_2pt(L, p1, p2, op, Q, xs)), (L, op)
+            assert _close(lat.nucleon_2pt(p1, p2, Q, xs), oracle.nucleon_2pt(L, p1, p2, Q, xs)), L
 
 
 def test_propagator_to_correlators_on_device(qkx, oracle):
@@ -82,5 +92,7 @@ def test_argument_checks(qkx):
             lat.meson_2pt(p, [10])
         with pytest.raises(qkx.QkxError):
             lat.baryon_2pt(p, p, 4)
+        with pytest.raises(qkx.QkxError):
+            lat.delta_2pt(p, p, 2)
         with pytest.raises(qkx.QkxError):
             lat.meson_2pt(p, [0], Q_sq=-1)

@@ -1,5 +1,6 @@
 """CPU tests of the contraction oracle (oracle/qkx_oracle_contract.c) against the
-reference's Meson/Baryon contractions and Fourier transforms: golden vectors
+reference's Meson/Baryon/Baryon_Dec contractions and Fourier transforms and its
+contractNucleon: golden vectors
 made from the compiled reference (tests/golden/ref_contract.npz) and the live
 build.  The restatement keeps the reference's term order and arithmetic, so
 agreement is to the last bit on the golden lattice."""
@@ -43,6 +44,20 @@ def test_contractions_golden(oracle):
         assert np.abs(a - g[f"baryon:{name}"]).max() <= 1e-14 * np.abs(a).max(), name
 
 
+def test_decuplet_and_contract_nucleon_golden(oracle):
+    """Baryon_Dec (both isospin operators) to the last bit; contractNucleon against the
+    numbers the reference printed (7 digits) and, to rounding, against Baryon NTN."""
+    g = _g()
+    L, p1, p2 = _props(oracle, g)
+    Q, xs = int(g["Q_sq"]), tuple(int(v) for v in g["x_src"])
+    for op, name in enumerate(oracle.DELTAS):
+        assert np.array_equal(oracle.delta_2pt(L, p1, p2, op, Q, xs), g[f"delta:{name}"]), name
+    n = oracle.nucleon_2pt(L, p1, p2, Q, xs)
+    scale = np.abs(n).max()
+    assert np.abs(n - g["nucleon_text"]).max() <= 1e-6 * scale
+    assert np.abs(n - g["baryon:NTN"]).max() <= 1e-14 * scale
+
+
 def test_contractions_vs_live_reference(oracle):
     if not oracle.ref_available():
         pytest.skip("reference build not present")
@@ -54,3 +69,5 @@ def test_contractions_vs_live_reference(oracle):
         for op in range(4):
             assert np.array_equal(oracle.baryon_2pt(L, p1, p2, op, Q, xs),
                                   oracle.ref_baryon_2pt(L, p1, p2, op, Q, xs))
+        for op in range(2):
+            assert np.array_equal(oracle.delta_2pt(L, p1, p2, op, Q, xs), oracle.ref_delta_2pt(L, p1, p2, op, Q, xs))
