@@ -443,13 +443,15 @@ def run_dslash(args):
     hops = {}
     with ClockSampler(0) as clk:
         for name, prec, S in (("fp16", Q.PREC_HALF, 52.0), ("fp32", Q.PREC_SINGLE, 96.0)):
-            nr, nt, ms = lat.tune(prec, NSRC)  # CUDA events around 3 pairs of Schur hops per tile, best tile
+            # CUDA events around 3 repetitions of the solver's four-hop iteration per tile, best tile
+            nr, nt, ms = lat.tune(prec, NSRC)
             table = lat.tune_table(prec, NSRC)
             best = min(table, key=lambda e: e["ms_per_hop"])["tile"]
-            # one output parity: input and output spinors, links shared by the batch, the
-            # xpay operand on every second hop of the pair
+            # one output parity, averaged over the four hops: input spinor and 8 links shared by the
+            # batch, the output spinor (hops 1-3), the xpay operand (hops 2 and 4), and the FP32 CG
+            # residual read and written by the fourth hop's epilogue
             G = hop_link_bytes({"fp16": "half", "fp32": "single"}[name], best)
-            nbytes = Vh * NSRC * (2.5 * S + 8.0 * G / NSRC)
+            nbytes = Vh * NSRC * ((9.0 * S + 2.0 * 96.0) / 4.0 + 8.0 * G / NSRC)
             hops[name] = {"tile": best, "ms_per_hop": ms, "gbs": nbytes / (ms * 1e-3) / 1e9,
                           "algorithmic_bytes_per_hop": nbytes,
                           "tiles_ms_per_hop": {",".join(map(str, e["tile"])): round(e["ms_per_hop"], 4)

@@ -261,11 +261,17 @@ QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, 
                    double* const* x_dev, qkx_solve_info* info);
 
 /* Many solves on several lattices at once (no reference counterpart).  Each
- * job is one qkx_invert_dev on its context (a lattice with its own links,
- * parameters and stream).  The jobs of a context run in order on one host
- * thread, different contexts on different threads, so their kernels overlap
- * on the GPU; contexts start in order of decreasing volume.  sp applies to
- * every job (its mu replaced by the job's). */
+ * job is a batch of right-hand sides on its context (a lattice with its own
+ * links, parameters and stream); sp applies to every job (its mu replaced by
+ * the job's).  For QKX_SOLVER_CG_EO_MIXED with use_graphs, the jobs of a
+ * context are merged into one batch (each right-hand side keeps its twisted
+ * mass) and every context's whole solve is one branch of a single CUDA graph:
+ * all lattices run from one launch and share the GPU, largest lattice first;
+ * a job's latency is when its lattice's branch ended, and its info is its
+ * lattice's (true_residual the worst of the job's own right-hand sides; the
+ * phase times are 0).  Otherwise the jobs of a context run in order on one
+ * host thread and different contexts on different threads, so their kernels
+ * overlap on the GPU; contexts start in order of decreasing volume. */
 typedef struct qkx_batch_job {
   qkx_ctx* ctx;                /* the job's lattice */
   int nrhs;                    /* right-hand sides of this job */

@@ -1,12 +1,16 @@
 // batch.cu -- many solves on several lattices at once (no reference
 // counterpart: the reference solves one system per MPI job).
 //
-// Each job is a batched solve (qkx_invert_dev) on some context; a context is
-// one lattice with its own links, parameters and CUDA stream.  The jobs of a
-// context run in order on one host thread and different contexts run on
-// different threads, so their kernels overlap on the GPU through their
-// streams.  Contexts start in order of decreasing volume (longest job
-// first), which bounds the makespan when lattices are uneven.
+// Each job is a batch of right-hand sides on some context; a context is one
+// lattice with its own links, parameters and CUDA stream.  For the even-odd
+// mixed solver with graphs on, the jobs of a context are merged into one batch
+// (each right-hand side with its own twisted mass) and every context's whole
+// solve is one branch of a single CUDA graph: one launch for all lattices
+// (invert_batch_graph, mixed.cu).  Otherwise the jobs of a context run in order
+// on one host thread and different contexts run on different threads, so their
+// kernels overlap on the GPU through their streams.  Either way contexts start
+// in order of decreasing volume (longest first), which bounds the makespan
+// when lattices are uneven.
 #include <stdio.h>
 
 #include <algorithm>
@@ -36,6 +40,17 @@ int qkx_invert_batch(qkx_batch_job* jobs, int njobs, const qkx_solver_params* sp
     if (std::find(ctxs.begin(), ctxs.end(), jobs[i].ctx) == ctxs.end()) ctxs.push_back(jobs[i].ctx);
   std::stable_sort(ctxs.begin(), ctxs.end(), [](qkx_ctx* a, qkx_ctx* b) { return a->V > b->V; });
   const auto t0 = std::chrono::steady_clock::now();
+  const int g = invert_batch_graph(jobs, njobs, sp,
+                                   std::chrono::duration<double>(t0.time_since_epoch()).count());
+  if (g < 0) return g;
+  if (g == 0) {
+    for (int i = 0; i < njobs; i++)
+      if (jobs[i].status != QKX_OK) {
+        set_error("job %d failed with status %d: %s", i, jobs[i].status, jobs[i].message);
+        return jobs[i].status;
+      }
+    return QKX_OK;
+  }
   std::vector<std::thread> threads;
   for (qkx_ctx* c : ctxs) {
     threads.emplace_back([=]() {

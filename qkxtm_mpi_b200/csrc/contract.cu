@@ -292,14 +292,25 @@ int delta_terms(const Gammas& g, DeltaTerms& t) {
 
 constexpr int DT_SITES = 8;  // sites per block of the decuplet kernel (48 threads a site)
 
+// The six permutations (a, b, c) of lib/contractions.cpp:14-19 in their order, two bits a
+// colour, six bits a permutation, as one constant (no table in memory); sign +1 for the first
+// three, -1 for the others.
+constexpr unsigned long long EPS_PACKED =
+    (0ull | 1ull << 2 | 2ull << 4) | (2ull | 0ull << 2 | 1ull << 4) << 6 | (1ull | 2ull << 2 | 0ull << 4) << 12 |
+    (2ull | 1ull << 2 | 0ull << 4) << 18 | (0ull | 2ull << 2 | 1ull << 4) << 24 | (1ull | 0ull << 2 | 2ull << 4) << 30;
+__device__ __forceinline__ int eps_at(int e, int j) { return (int)((EPS_PACKED >> (6 * e + 2 * j)) & 3ull); }
+
 // C[i*16 + gamma*4 + gamma'][site] of Baryon_Dec::contract (lib/contractions.cpp:768-866):
 // one thread per (site, i, gamma, gamma'); op 0 DELTA_ISO1 (three quarks of p1),
 // 1 DELTA_ISO1O2 (p2 for the odd quark, the reference's weights 1/3 x {4, 2, 1}).
 // Each term reads its colour entries from the staged site blocks.
+// Every index the kernel takes from its term table is checked before use: a value out of range
+// records a code in *err and the term is skipped, so a bad table cannot address outside the
+// staged blocks.
 __global__ void __launch_bounds__(DT_SITES * 48) k_delta_sites(const double2* __restrict__ p1,
                                                                const double2* __restrict__ p2, size_t V, int op,
                                                                const DeltaTerms* __restrict__ T,
-                                                               double2* __restrict__ C) {
+                                                               double2* __restrict__ C, int* __restrict__ err) {
   extern __shared__ double2 sb[];
   double2* s1 = sb;
   double2* s2 = sb + DT_SITES * CT_STRIDE;
@@ -316,16 +327,24 @@ __global__ void __launch_bounds__(DT_SITES * 48) k_delta_sites(const double2* __
   // entry [s1][s2][c1][c2] of propagator q
   auto at = [](const double2* q, int sa, int sb_, int ca, int cb) { return q[sa * 36 + sb_ * 9 + ca * 3 + cb]; };
   double2 m = make_double2(0.0, 0.0);
-  const int n = T->n[i];
+  int n = T->n[i];
+  if (n < 0 || n > DELTA_MAX_TERMS) {
+    atomicCAS(err, 0, 1000 + n);
+    n = 0;
+  }
   for (int idx = 0; idx < n; idx++) {
     const double2 val = T->val[i][idx];
     const char4 ab = T->ab[i][idx];
     const int al = ab.x, be = ab.y, bp = ab.z, ap = ab.w;
+    if ((unsigned)al > 3u || (unsigned)be > 3u || (unsigned)bp > 3u || (unsigned)ap > 3u) {
+      atomicCAS(err, 0, 2000 + idx);
+      continue;
+    }
     for (int e1 = 0; e1 < 6; e1++) {
-      const int a = c_eps[e1][0], b = c_eps[e1][1], c = c_eps[e1][2];
+      const int a = eps_at(e1, 0), b = eps_at(e1, 1), c = eps_at(e1, 2);
       for (int e2 = 0; e2 < 6; e2++) {
-        const int a1 = c_eps[e2][0], b1 = c_eps[e2][1], c1 = c_eps[e2][2];
-        const double f = (double)(c_sgn[e1] * c_sgn[e2]);
+        const int a1 = eps_at(e2, 0), b1 = eps_at(e2, 1), c1 = eps_at(e2, 2);
+        const double f = (e1 < 3) == (e2 < 3) ? 1.0 : -1.0;
         double2 t;
         if (op == 0) {
           const double2 t1 = cm(cm(at(q1, al, gp, a, c1), at(q1, be, bp, b, b1)), at(q1, g, ap, c, a1));
@@ -534,8 +553,11 @@ int delta_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op,
   QKX_TRY(prop_in(c, p2, host, b));
   DeltaTerms* dT = nullptr;
   double2* C = nullptr;
+  int* derr = nullptr;
   QKX_CUDA(cudaMallocAsync((void**)&dT, sizeof(DeltaTerms), c->st));
   QKX_CUDA(cudaMallocAsync((void**)&C, sizeof(double2) * 48 * c->V, c->st));
+  QKX_CUDA(cudaMallocAsync((void**)&derr, sizeof(int), c->st));
+  QKX_CUDA(cudaMemsetAsync(derr, 0, sizeof(int), c->st));
   QKX_CUDA(cudaMemcpyAsync(dT, &T, sizeof(DeltaTerms), cudaMemcpyHostToDevice, c->st));
   static bool attr = false;
   const int smem = (int)(sizeof(double2) * 2 * DT_SITES * CT_STRIDE);
@@ -544,9 +566,22 @@ int delta_2pt(qkx_ctx* c, const double* p1, const double* p2, bool host, int op,
     attr = true;
   }
   const unsigned nb = (unsigned)((c->V + DT_SITES - 1) / DT_SITES);
-  k_delta_sites<<<nb, DT_SITES * 48, smem, c->st>>>(a.d, b.d, c->V, op, dT, C);
+  k_delta_sites<<<nb, DT_SITES * 48, smem, c->st>>>(a.d, b.d, c->V, op, dT, C, derr);
   counted(c);
   QKX_CUDA(cudaGetLastError());
+  int herr = 0;
+  QKX_CUDA(cudaMemcpyAsync(&herr, derr, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+  cudaFreeAsync(derr, c->st);
+  if (herr != 0) {
+    set_error("decuplet kernel: bad spin-term table entry (code %d)", herr);
+    cudaFreeAsync(dT, c->st);
+    cudaFreeAsync(C, c->st);
+    if (a.owned) cudaFreeAsync(a.owned, c->st);
+    if (b.owned) cudaFreeAsync(b.owned, c->st);
+    cudaStreamSynchronize(c->st);
+    return QKX_ERR_CUDA;
+  }
   // Baryon_Dec::F is [Lt][Nmom][3][4][4]: one transform of 16 components per i, interleaved
   const size_t per = (size_t)c->p.L[3] * nmom * 16;
   std::vector<double> tmp(2 * per);

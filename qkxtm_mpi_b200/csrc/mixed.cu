@@ -30,6 +30,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <chrono>
+#include <memory>
 #include <type_traits>
 #include <vector>
 
@@ -369,6 +371,7 @@ struct MxCtl {
   int nan_rhs, nan_iter;   // first right-hand side whose r^2 became NaN or inf, and when (0: none)
   int unconverged;         // right-hand sides still active when the loop ended
   unsigned long long t_ru0, ru_ns;  // device clock at the start of the last update; summed update time
+  double cv[MAX_RHS], sv[MAX_RHS];  // per-RHS twist factors, staged here (page-locked) for the set-up's copies
 };
 
 __device__ __forceinline__ unsigned long long mx_clock_ns() {
@@ -481,11 +484,13 @@ __global__ void __launch_bounds__(MAX_RHS) k_ctl_final(CgScalars* sc, MxCtl* ctl
   if (i == 0) ctl->unconverged = n;
 }
 
-// Builds the loop graph into `top`: emit(part, h_outer, h_inner) launches the kernels of each
-// part on the context's stream while it is being captured (0: top level before the outer loop,
-// 1: outer body before the inner loop, 2: outer body after it, 3: inner body).  The kernels each
-// part launched come back in *kt, *ko, *ki.  Both handles default to 0 at every launch, so a
-// loop whose condition is never set does not run.
+// Builds the loop graph into `top` (which may already hold other work: the new nodes are roots
+// of their own branch): emit(part, h_outer, h_inner) launches the kernels of each part on the
+// context's stream while it is being captured (-1: top level, before anything else of the
+// branch; 0: top level before the outer loop; 4: top level after it; 1: outer body before the
+// inner loop; 2: outer body after it; 3: inner body).  The kernels each level launched come back
+// in *kt, *ko, *ki.  Both handles default to 0 at every launch, so a loop whose condition is never
+// set does not run.
 template <class Emit>
 static int build_loop_graph(qkx_ctx* c, cudaGraph_t top, long long* kt, long long* ko, long long* ki, Emit emit) {
   bool capturing = false;
@@ -531,8 +536,10 @@ static int build_loop_graph(qkx_ctx* c, cudaGraph_t top, long long* kt, long lon
     cudaGraph_t outer_body = nullptr, inner_body = nullptr;
     QKX_CUDA(cudaGraphConditionalHandleCreate(&h_outer, top, 0, cudaGraphCondAssignDefault));
     QKX_TRY(begin(top));
+    QKX_TRY(emit(-1, h_outer, h_inner));
     QKX_TRY(emit(0, h_outer, h_inner));
     QKX_TRY(add_while(h_outer, &outer_body));
+    QKX_TRY(emit(4, h_outer, h_inner));
     QKX_TRY(end(kt));
     QKX_CUDA(cudaGraphConditionalHandleCreate(&h_inner, outer_body, 0, cudaGraphCondAssignDefault));
     QKX_TRY(begin(outer_body));
@@ -842,9 +849,10 @@ GaugeF64x18 Sloppy<PDouble>::gauge(qkx_ctx* c) {
 }
 
 // ---------------------------------------------------------------- autotuner
-// Times the two inner hop shapes (TWIST_INV then XPAY_G5 with the fused norm)
-// for every tile on this lattice and batch, on the solver's own fields, and
-// keeps the fastest.  The result is cached in the context per (precision,
+// Times the four hops of an inner iteration as the solver runs them (TWIST_INV,
+// XPAY_G5 with the fused norm, TWIST_INV, and XPAY_G5 feeding the CG residual
+// update) for every tile on this lattice and batch, on the solver's own fields,
+// and keeps the fastest.  The result is cached in the context per (precision,
 // batch size) and survives gauge reloads.
 template <class P>
 static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
@@ -854,14 +862,17 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
   using FT = FieldTraits<SP>;
   MixedState* m = c->mixed;
   const int Vh = c->Vh;
-  SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh);
+  using FA = FieldTraits<typename P::AC>;
+  SP p = FT::acc(m->p, 0, Vh), t = FT::acc(m->t, 1, Vh), y = FT::acc(m->y, 0, Vh), Ap = FT::acc(m->Ap, 0, Vh);
   const GA U = Sloppy<P>::gauge(c);
   const Geom g = Sloppy<P>::geom(c);
   CgScalars* sh = c->sc_h;
   for (int i = 0; i < MAX_RHS; i++) sh->active[i] = i < R_ ? 1 : 0;
   QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+  QKX_CUDA(cudaMemsetAsync(c->sc->alpha, 0, sizeof(double) * MAX_RHS, c->st));
   QKX_CUDA(cudaMemsetAsync(m->p.d, 0, FT::words * 16 * (size_t)Vh * R_, c->st));
   if (m->p.n) QKX_CUDA(cudaMemsetAsync(m->p.n, 0, sizeof(float) * (size_t)Vh * R_, c->st));
+  QKX_CUDA(cudaMemsetAsync(m->rs.d, 0, FA::words * 16 * (size_t)Vh * R_, c->st));
   cudaEvent_t e0, e1;
   QKX_CUDA(cudaEventCreate(&e0));
   QKX_CUDA(cudaEventCreate(&e1));
@@ -879,6 +890,10 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
         rc = hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, p, t, p, 1, 0.0, 1.0, true, nullptr, -1);
       if (rc == QKX_OK)
         rc = hop_tile<SP, GA, R, EPI_XPAY_G5>(c, tile, R_, U, g, t, y, p, 0, -k2, 1.0, false, m->part, -1);
+      if (rc == QKX_OK)
+        rc = hop_tile<SP, GA, R, EPI_TWIST_INV>(c, tile, R_, U, g, y, t, y, 1, 0.0, -1.0, true, nullptr, -1);
+      if (rc == QKX_OK)
+        rc = hop_tile<SP, GA, R, EPI_XPAY_G5_CGR>(c, tile, R_, U, g, t, Ap, y, 0, -k2, -1.0, false, m->part, -1);
     }
     if (rc != QKX_OK) break;
     if (cudaEventRecord(e1, c->st) != cudaSuccess || cudaEventSynchronize(e1) != cudaSuccess) {
@@ -887,7 +902,7 @@ static int tune_tile(qkx_ctx* c, int R_, HopTile* best, double* best_ms) {
     }
     float ms = 0;
     cudaEventElapsedTime(&ms, e0, e1);
-    const double per_hop = ms / 6.0;
+    const double per_hop = ms / 12.0;
     log.push_back({double(tile.nr), double(tile.nt), double(tile.kind), per_hop});
     if (per_hop < *best_ms) {
       *best_ms = per_hop;
@@ -970,106 +985,140 @@ static int normal_residual_f32(qkx_ctx* c, int R_, double2* z, SpinorF32 out, in
   return normal_residual_from32(c, R_, out, nblk);
 }
 
+// One even-odd mixed solve, in phases, so that a single solve can run them eagerly and a batch of
+// lattices can capture the set-up, loop and final phase of each into one graph (qkx_invert_batch).
+//   prepare()       allocation, tile, per-RHS twist factors and scalars into page-locked memory
+//   setup()         b^, |b|^2, Mh^+ b^ and the starting fields, on the context's stream (capturable)
+//   loop_graph()    the device-driven iteration loop added to a graph
+//   host_loop()     the host-driven loop (hop kernels timed with events, or graphs off)
+//   final_phase()   odd sites, the FP64 true residual, solutions out, scalars to the host (capturable)
+//   finish()        solve info and status from the scalars the final phase copied back
 template <class P>
-static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
-                             double2* const* x, qkx_solve_info* info) {
+struct MixedSolve {
   using SL = Sloppy<P>;
   using SP = typename P::SP;
   using AC = typename P::AC;
   using R = typename P::R;
   using FT = FieldTraits<SP>;
   using FA = FieldTraits<AC>;
-  QKX_TRY(mixed_alloc<P>(c, nrhs, true));
-  MixedState* m = c->mixed;
+  static constexpr bool r32 = std::is_same<AC, SpinorF32>::value;
+
+  qkx_ctx* c;
+  const qkx_solver_params* sp;
+  int nrhs;
+  const double2* const* b;
+  double2* const* x;
+  MixedState* m = nullptr;
   HopTile tile;
-  QKX_TRY(tile_for<P>(c, nrhs, &tile));
-  const int Vh = c->Vh;
-  const size_t n12 = 12 * (size_t)Vh;
-  const size_t hb = sizeof(double2) * n12;
-  const double k = c->p.kappa, ts = c->p.twistSign;
-  const double delta =
-      sp->reliable_delta > 0 ? std::max(P::delta_min, std::min(0.5, sp->reliable_delta)) : P::delta;
-  const int nblk = hop_blocks_per_rhs<128>(Vh, 0);
-  const int cgrid = (Vh + 255) / 256;
-  const dim3 cg2(cgrid, nrhs), bg2(MX_GRID, nrhs);
-  const H18 U18{c->U18, Vh};
+  int Vh = 0;
+  size_t n12 = 0, hb = 0;
+  double k = 0, delta = 0, target = 0;
+  int maxIter = 0;
+  dim3 cg2, bg2;
+  bool device_loop = false;
+  long long kcount[3] = {};  // kernels of the loop graph's top level, outer pass and inner pass
+  // results of the host-driven loop (the device loop keeps them in MxCtl)
+  int iter = 0, n_ru = 0, n_restart = 0, diverged = 0, nact = 0;
+  float ms_ru = 0;
+  std::vector<int> active;
+  std::vector<double> bnorm2;
 
-  std::vector<double> mus(nrhs), cv(nrhs), sv(nrhs);
-  for (int i = 0; i < nrhs; i++) {
-    mus[i] = sp->mu ? sp->mu[i] : c->p.mu;
-    cv[i] = 2.0 * k * mus[i] * ts;
-    sv[i] = 1.0 / (1.0 + (2.0 * k * mus[i]) * (2.0 * k * mus[i]));
+  MixedSolve(qkx_ctx* c_, const qkx_solver_params* sp_, int nrhs_, const double2* const* b_, double2* const* x_)
+      : c(c_), sp(sp_), nrhs(nrhs_), b(b_), x(x_), active(nrhs_, 1), bnorm2(nrhs_) {}
+
+  int prepare(bool allow_device_loop) {
+    QKX_TRY(mixed_alloc<P>(c, nrhs, true));
+    m = c->mixed;
+    QKX_TRY(tile_for<P>(c, nrhs, &tile));
+    Vh = c->Vh;
+    n12 = 12 * (size_t)Vh;
+    hb = sizeof(double2) * n12;
+    k = c->p.kappa;
+    const double ts = c->p.twistSign;
+    delta = sp->reliable_delta > 0 ? std::max(P::delta_min, std::min(0.5, sp->reliable_delta)) : P::delta;
+    target = 0.9 * sp->tol;
+    maxIter = std::min(sp->maxIter, 1000000);
+    cg2 = dim3((Vh + 255) / 256, nrhs);
+    bg2 = dim3(MX_GRID, nrhs);
+    // the whole iteration loop on the device (one graph launch) unless the hop kernels are being
+    // timed one by one (event records cannot sit inside a conditional graph body) or graphs are off
+    device_loop = allow_device_loop && sp->use_graphs != 0 && c->prof == 0;
+    MxCtl* hc = m->ctl_h;
+    memset(hc, 0, sizeof(MxCtl));
+    hc->nrhs = nrhs;
+    hc->maxIter = maxIter;
+    hc->delta2 = delta * delta;
+    hc->target2 = target * target;
+    for (int i = 0; i < nrhs; i++) {
+      const double mu = sp->mu ? sp->mu[i] : c->p.mu;
+      hc->cv[i] = 2.0 * k * mu * ts;
+      hc->sv[i] = 1.0 / (1.0 + (2.0 * k * mu) * (2.0 * k * mu));
+    }
+    CgScalars* sh = c->sc_h;
+    memset(sh, 0, sizeof(CgScalars));
+    for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
+    for (auto& e : m->ph)
+      if (!e) QKX_CUDA(cudaEventCreate(&e));
+    return QKX_OK;
   }
-  CgScalars* sh = c->sc_h;
-  memset(sh, 0, sizeof(CgScalars));
-  for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
-  for (auto& e : m->ph)
-    if (!e) QKX_CUDA(cudaEventCreate(&e));
-
-  QKX_CUDA(cudaEventRecord(c->t0, c->st));
-  QKX_CUDA(cudaMemcpyAsync(m->cvec, cv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
-  QKX_CUDA(cudaMemcpyAsync(m->svec, sv.data(), sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
-  QKX_CUDA(cudaMemcpyAsync(c->sc, sh, sizeof(CgScalars), cudaMemcpyHostToDevice, c->st));
 
   // --- set-up, batched FP64: gather b, |b|^2; b^_e = b_e + k D_eo A^-1 b_o; g5 b^_e; r = Mh^+ b^_e
-  for (int i = 0; i < nrhs; i++) {
-    QKX_CUDA(cudaMemcpyAsync(m->bE + i * n12, b[i], hb, cudaMemcpyDeviceToDevice, c->st));
-    QKX_CUDA(cudaMemcpyAsync(m->bO + i * n12, b[i] + n12, hb, cudaMemcpyDeviceToDevice, c->st));
-  }
-  k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), m->part);
-  counted(c);
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
-  counted(c);
-  k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), m->part);
-  counted(c);
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
-  counted(c);
-  // t_o = A^-1 b_o
-  k_mx_site<SITE_TWIST_INV><<<cg2, 256, 0, c->st>>>(B64(m->bO, 1, Vh), B64(m->t64, 1, Vh), 1, m->cvec, m->svec);
-  counted(c);
-  QKX_CUDA(cudaGetLastError());
-  // z = b_e + k D_eo t_o = b^_e, |b^|^2 -> aux2 ; g5bh = g5 b^_e
-  int nb64 = 0;
-  QKX_TRY(hop64_batch(c, EPI_XPAY, nrhs, B64(m->t64, 1, Vh), B64(m->z64, 0, Vh), B64(m->bE, 0, Vh), 0, k, 0.0,
-                      m->cvec, nullptr, c->sc->active, m->part, &nb64));
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
-  counted(c);
-  k_mx_site<SITE_GAMMA5><<<cg2, 256, 0, c->st>>>(B64(m->z64, 0, Vh), B64(m->g5bh, 0, Vh), 0, nullptr, nullptr);
-  counted(c);
-  // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2 (FP32 when the sloppy residual is FP32)
-  constexpr bool r32 = std::is_same<AC, SpinorF32>::value;
-  if constexpr (r32) {
-    QKX_TRY(normal_residual_f32(c, nrhs, m->g5bh, FA::acc(m->rs, 0, Vh), &nb64));
-  } else {
-    QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part, &nb64));
-  }
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_R2_INIT, c->sc);
-  counted(c);
-  QKX_CUDA(cudaMemsetAsync(m->x64, 0, hb * nrhs, c->st));
-  QKX_CUDA(cudaMemsetAsync(m->xs.d, 0, FA::words * 16 * (size_t)Vh * nrhs, c->st));
-  if constexpr (r32) {
-    k_mx_convert<AC, SP><<<cg2, 256, 0, c->st>>>(FA::acc(m->rs, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+  int setup() {
+    MxCtl* hc = m->ctl_h;
+    QKX_CUDA(cudaMemcpyAsync(m->cvec, hc->cv, sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(m->svec, hc->sv, sizeof(double) * nrhs, cudaMemcpyHostToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(c->sc, c->sc_h, sizeof(CgScalars), cudaMemcpyHostToDevice, c->st));
+    if (device_loop) QKX_CUDA(cudaMemcpyAsync(m->ctl, hc, sizeof(MxCtl), cudaMemcpyHostToDevice, c->st));
+    for (int i = 0; i < nrhs; i++) {
+      QKX_CUDA(cudaMemcpyAsync(m->bE + i * n12, b[i], hb, cudaMemcpyDeviceToDevice, c->st));
+      QKX_CUDA(cudaMemcpyAsync(m->bO + i * n12, b[i] + n12, hb, cudaMemcpyDeviceToDevice, c->st));
+    }
+    k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bE, 0, Vh), m->part);
     counted(c);
-  } else {
-    k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
     counted(c);
-    k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+    k_mx_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->bO, 0, Vh), m->part);
     counted(c);
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX_ADD, c->sc);
+    counted(c);
+    // t_o = A^-1 b_o
+    k_mx_site<SITE_TWIST_INV><<<cg2, 256, 0, c->st>>>(B64(m->bO, 1, Vh), B64(m->t64, 1, Vh), 1, m->cvec, m->svec);
+    counted(c);
+    QKX_CUDA(cudaGetLastError());
+    // z = b_e + k D_eo t_o = b^_e, |b^|^2 -> aux2 ; g5bh = g5 b^_e
+    int nb64 = 0;
+    QKX_TRY(hop64_batch(c, EPI_XPAY, nrhs, B64(m->t64, 1, Vh), B64(m->z64, 0, Vh), B64(m->bE, 0, Vh), 0, k, 0.0,
+                        m->cvec, nullptr, c->sc->active, m->part, &nb64));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_AUX2, c->sc);
+    counted(c);
+    k_mx_site<SITE_GAMMA5><<<cg2, 256, 0, c->st>>>(B64(m->z64, 0, Vh), B64(m->g5bh, 0, Vh), 0, nullptr, nullptr);
+    counted(c);
+    // r = g5 Mh(-c) g5 b^_e = Mh^+ b^_e, |r|^2 -> r2 (FP32 when the sloppy residual is FP32)
+    if constexpr (r32) {
+      QKX_TRY(normal_residual_f32(c, nrhs, m->g5bh, FA::acc(m->rs, 0, Vh), &nb64));
+    } else {
+      QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->g5bh, m->r64, m->part, &nb64));
+    }
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nb64, FIN_R2_INIT, c->sc);
+    counted(c);
+    QKX_CUDA(cudaMemsetAsync(m->x64, 0, hb * nrhs, c->st));
+    QKX_CUDA(cudaMemsetAsync(m->xs.d, 0, FA::words * 16 * (size_t)Vh * nrhs, c->st));
+    if constexpr (r32) {
+      k_mx_convert<AC, SP><<<cg2, 256, 0, c->st>>>(FA::acc(m->rs, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+      counted(c);
+    } else {
+      k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), nullptr);
+      counted(c);
+      k_mx_from_f64<SP, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FT::acc(m->p, 0, Vh), nullptr);
+      counted(c);
+    }
+    QKX_CUDA(cudaGetLastError());
+    return QKX_OK;
   }
-  QKX_CUDA(cudaGetLastError());
-  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));  // set-up done
-
-  const bool prof = c->prof != 0;
-  const bool graphs = sp->use_graphs != 0;
-  // the whole iteration loop on the device (one graph launch) unless the hop kernels are being
-  // timed one by one (event records cannot sit inside a conditional graph body) or graphs are off
-  const bool device_loop = graphs && !prof;
-  const int maxIter = std::min(sp->maxIter, 1000000);
-  const double target = 0.9 * sp->tol;
 
   // reliable update of the active RHS: x64 += x_s (x_s = 0); the FP64 true residual
   // |rhat|^2 -> aux; the residual the sloppy CG restarts from, Mh^+ rhat, with its norm -> aux2
-  auto reliable_update = [&]() -> int {
+  int reliable_update() {
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
     counted(c);
     int nb = 0;
@@ -1097,10 +1146,11 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     counted(c);
     QKX_CUDA(cudaGetLastError());
     return QKX_OK;
-  };
+  }
+
   // after an update's decisions (active and restart flags set): the sloppy residual of the RHS
   // that go on, and p = r where the search direction restarts
-  auto restart_kernels = [&](bool any_restart) -> int {
+  int restart_kernels(bool any_restart) {
     if constexpr (!r32) {
       k_mx_from_f64<AC, R><<<cg2, 256, 0, c->st>>>(B64(m->r64, 0, Vh), FA::acc(m->rs, 0, Vh), c->sc->active);
       counted(c);
@@ -1111,25 +1161,45 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
     }
     QKX_CUDA(cudaGetLastError());
     return QKX_OK;
-  };
+  }
 
-  float ms_setup = 0, ms_ru = 0, ms_seg = 0;
-  int iter = 0, n_ru = 0, n_restart = 0, diverged = 0;
-  std::vector<int> active(nrhs, 1);
-  std::vector<double> bnorm2(nrhs);  // |b|^2 per RHS
-  MxCtl* hc = m->ctl_h;
+  // --- the iteration loop as a graph: WHILE (any RHS active) { WHILE (no reliable update asked
+  // for) { iteration }; reliable update; decisions }, added to `top`.  Every decision of the host
+  // loop is taken by a one-block kernel from the same scalars; both loops are bounded by maxIter
+  // because every pass of the outer one runs at least one inner iteration.  pre / post emit work
+  // into the top level before and after the loop (the batch's set-up and final phase).
+  template <class Pre, class Post>
+  int loop_graph(cudaGraph_t top, long long* kt, long long* ko, long long* ki, Pre pre, Post post) {
+    return build_loop_graph(c, top, kt, ko, ki,
+                            [&](int part, cudaGraphConditionalHandle h_outer, cudaGraphConditionalHandle h_inner) -> int {
+                              if (part == -1) return pre();
+                              if (part == 4) return post();
+                              if (part == 0) {  // per-RHS state from the set-up
+                                k_ctl_start<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
+                                counted(c);
+                                return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+                              }
+                              if (part == 1) {  // outer body before the inner loop
+                                k_ctl_inner_begin<<<1, 1, 0, c->st>>>(h_inner);
+                                counted(c);
+                                return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+                              }
+                              if (part == 2) {  // outer body after the inner loop
+                                QKX_TRY(reliable_update());
+                                k_ctl_after_ru<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
+                                counted(c);
+                                return restart_kernels(true);
+                              }
+                              // inner body: one iteration and the decision to go on
+                              QKX_TRY(SL::iteration(c, nrhs, false, tile));
+                              k_ctl_after_iter<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_inner);
+                              counted(c);
+                              return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
+                            });
+  }
 
-  if (device_loop) {
-    // --- the iteration loop as one graph: WHILE (any RHS active) { WHILE (no reliable update
-    // asked for) { iteration }; reliable update; decisions }.  Every decision of the host loop
-    // below is taken by a one-block kernel from the same scalars; both loops are bounded by
-    // maxIter because every pass of the outer one runs at least one inner iteration.
-    memset(hc, 0, sizeof(MxCtl));
-    hc->nrhs = nrhs;
-    hc->maxIter = maxIter;
-    hc->delta2 = delta * delta;
-    hc->target2 = target * target;
-    QKX_CUDA(cudaMemcpyAsync(m->ctl, hc, sizeof(MxCtl), cudaMemcpyHostToDevice, c->st));
+  // the loop graph of this context (cached while the batch size, kappa and tile stay), launched
+  int device_loop_launch() {
     if (m->dgraph && (m->dgraph_R != nrhs || m->dgraph_kappa != c->p.kappa || m->dgraph_nr != tile.nr ||
                       m->dgraph_nt != tile.nt || m->dgraph_kind != tile.kind)) {
       QKX_CUDA(cudaStreamSynchronize(c->st));
@@ -1140,30 +1210,8 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
       cudaGraph_t top = nullptr;
       QKX_CUDA(cudaGraphCreate(&top, 0));
       long long kt = 0, ko = 0, ki = 0;
-      int rc = build_loop_graph(c, top, &kt, &ko, &ki, [&](int part, cudaGraphConditionalHandle h_outer,
-                                                           cudaGraphConditionalHandle h_inner) -> int {
-        if (part == 0) {  // top level: per-RHS state from the set-up
-          k_ctl_start<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
-          counted(c);
-          return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
-        }
-        if (part == 1) {  // outer body before the inner loop
-          k_ctl_inner_begin<<<1, 1, 0, c->st>>>(h_inner);
-          counted(c);
-          return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
-        }
-        if (part == 2) {  // outer body after the inner loop
-          QKX_TRY(reliable_update());
-          k_ctl_after_ru<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_outer);
-          counted(c);
-          return restart_kernels(true);
-        }
-        // inner body: one iteration and the decision to go on
-        QKX_TRY(SL::iteration(c, nrhs, false, tile));
-        k_ctl_after_iter<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl, h_inner);
-        counted(c);
-        return cudaGetLastError() == cudaSuccess ? QKX_OK : QKX_ERR_CUDA;
-      });
+      auto none = []() -> int { return QKX_OK; };
+      int rc = loop_graph(top, &kt, &ko, &ki, none, none);
       if (rc == QKX_OK) {
         const cudaError_t e = cudaGraphInstantiate(&m->dgraph, top, 0);
         if (e != cudaSuccess) {
@@ -1183,9 +1231,17 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
       m->dgraph_k[1] = ko;
       m->dgraph_k[2] = ki;
     }
+    for (int i = 0; i < 3; i++) kcount[i] = m->dgraph_k[i];
     QKX_CUDA(cudaGraphLaunch(m->dgraph, c->st));
-  } else {
-    // --- host-driven loop: the host reads r^2 after every iteration and takes the decisions
+    return QKX_OK;
+  }
+
+  // --- host-driven loop: the host reads r^2 after every iteration and takes the decisions
+  int host_loop() {
+    CgScalars* sh = c->sc_h;
+    const bool prof = c->prof != 0;
+    const bool graphs = sp->use_graphs != 0;
+    float ms_seg = 0;
     QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
     QKX_CUDA(cudaStreamSynchronize(c->st));
     bool ru_pending = false;  // a reliable update's end mark not yet read
@@ -1241,9 +1297,9 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
 
     int since = 0;
     while (iter < maxIter) {
-      int nact = 0;
-      for (int i = 0; i < nrhs; i++) nact += active[i];
-      if (!nact) break;
+      int na = 0;
+      for (int i = 0; i < nrhs; i++) na += active[i];
+      if (!na) break;
       if (m->graph) {
         QKX_CUDA(cudaGraphLaunch(m->graph, c->st));
         counted(c, (int)m->graph_kernels);
@@ -1265,7 +1321,7 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
           QKX_CUDA(cudaEventElapsedTime(&ms, m->gev[2 * h], m->gev[2 * h + 1]));
           c->prof_ms += ms;
           c->prof_launches++;
-          c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs, tile) * nact;
+          c->prof_bytes += SL::hop_bytes_per_rhs(c, nrhs, tile) * na;
         }
       }
       // reliable update of every active RHS when one of them asks for it
@@ -1331,91 +1387,272 @@ static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, 
       QKX_CUDA(cudaEventElapsedTime(&ms_seg, m->ph[1], m->ph[2]));
       ms_ru += ms_seg;
     }
-  }
-
-  // --- odd parity and the FP64 true residual of the full system, batched, for every RHS
-  // the final phase starts where the loop ended
-  QKX_CUDA(cudaEventRecord(m->ph[3], c->st));
-  int nact = 0;
-  if (device_loop) {
-    k_ctl_final<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl);
-    counted(c);
-  } else {
     for (int i = 0; i < nrhs; i++) nact += active[i];
+    // every RHS takes part in the final phase
     for (int i = 0; i < nrhs; i++) sh->active[i] = 1;
     QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+    return QKX_OK;
   }
-  // fold what the unconverged RHS accumulated since their last update (x_s is zero for the others)
-  if (device_loop || nact) {
-    k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+
+  // --- odd parity and the FP64 true residual of the full system, batched, for every RHS;
+  // the solutions to x[] and the scalars to the host mirrors
+  int final_phase() {
+    if (device_loop) {
+      k_ctl_final<<<1, MAX_RHS, 0, c->st>>>(c->sc, m->ctl);
+      counted(c);
+    }
+    // fold what the unconverged RHS accumulated since their last update (x_s is zero for the others)
+    if (device_loop || nact) {
+      k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
+      counted(c);
+    }
+    // x_o = A^-1 (b_o + k D_oe x_e) into t64
+    QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
+                        m->cvec, m->svec, c->sc->active, nullptr, nullptr));
+    // ||b - M x||^2 on the full lattice (x: even half in x64, odd half in t64), summed in FP64 by the
+    // hop's epilogue; nothing is stored
+    int nbr = 0;
+    QKX_TRY(hop64_batch_res(c, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->x64, m->t64, Vh),
+                            B64full(m->bE, m->bO, Vh), SpinorF32{nullptr, nullptr, Vh}, -1, -k, 1.0, m->cvec,
+                            c->sc->active, m->part, &nbr, false));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbr, FIN_AUX, c->sc);
     counted(c);
+    QKX_CUDA(cudaGetLastError());
+    for (int i = 0; i < nrhs; i++) {
+      QKX_CUDA(cudaMemcpyAsync(x[i], m->x64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
+      QKX_CUDA(cudaMemcpyAsync(x[i] + n12, m->t64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
+    }
+    QKX_CUDA(cudaMemcpyAsync(c->sc_h, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
+    if (device_loop) QKX_CUDA(cudaMemcpyAsync(m->ctl_h, m->ctl, sizeof(MxCtl), cudaMemcpyDeviceToHost, c->st));
+    return QKX_OK;
   }
-  // x_o = A^-1 (b_o + k D_oe x_e) into t64
-  QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
-                      m->cvec, m->svec, c->sc->active, nullptr, nullptr));
-  // ||b - M x||^2 on the full lattice (x: even half in x64, odd half in t64), summed in FP64 by the
-  // hop's epilogue; nothing is stored
-  int nbr = 0;
-  QKX_TRY(hop64_batch_res(c, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->x64, m->t64, Vh),
-                          B64full(m->bE, m->bO, Vh), SpinorF32{nullptr, nullptr, Vh}, -1, -k, 1.0, m->cvec,
-                          c->sc->active, m->part, &nbr, false));
-  k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbr, FIN_AUX, c->sc);
-  counted(c);
-  QKX_CUDA(cudaGetLastError());
-  for (int i = 0; i < nrhs; i++) {
-    QKX_CUDA(cudaMemcpyAsync(x[i], m->x64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
-    QKX_CUDA(cudaMemcpyAsync(x[i] + n12, m->t64 + i * n12, hb, cudaMemcpyDeviceToDevice, c->st));
+
+  // status and solve info once the final phase's copies are in host memory; rel (optional) gets
+  // every RHS's true residual ||b - M x|| / ||b||.  Device times: the phase marks when given.
+  int finish(qkx_solve_info* info, double* rel, const float* ms_total, const float* ms_setup, const float* ms_final) {
+    CgScalars* sh = c->sc_h;
+    if (device_loop) {
+      MxCtl* hc = m->ctl_h;
+      iter = hc->iter;
+      n_ru = hc->n_ru;
+      n_restart = hc->n_restart;
+      diverged = hc->diverged;
+      nact = hc->unconverged;
+      ms_ru = float(hc->ru_ns * 1e-6);
+      for (int i = 0; i < nrhs; i++) bnorm2[i] = hc->bnorm2[i];
+      counted(c, (int)(kcount[0] + (long long)hc->n_outer * kcount[1] + (long long)hc->iter * kcount[2]));
+      if (hc->nan_iter > 0) {
+        set_error("mixed CG: r2 of right-hand side %d became non-finite at iteration %d", hc->nan_rhs, hc->nan_iter);
+        return QKX_ERR_NAN;
+      }
+    }
+    int rc = nact ? QKX_ERR_NOT_CONVERGED : QKX_OK;
+    double worst = 0.0;
+    int it = 0;
+    for (int i = 0; i < nrhs; i++) {
+      const double r = bnorm2[i] > 0 ? sqrt(sh->aux[i] / bnorm2[i]) : 0.0;
+      if (rel) rel[i] = r;
+      worst = std::max(worst, r);
+      it = std::max(it, sh->iters[i]);
+    }
+    if (rc == QKX_OK && worst > sp->tol) rc = QKX_ERR_NOT_CONVERGED;
+    if (info) {
+      info->iterations = it;
+      info->reliable_updates = n_ru;
+      info->restarts = n_restart;
+      info->converged = rc == QKX_OK;
+      info->true_residual = worst;
+      info->normal_residual = 0.0;
+      info->seconds = ms_total ? *ms_total * 1e-3 : 0.0;
+      info->seconds_setup = ms_setup ? *ms_setup * 1e-3 : 0.0;
+      info->seconds_reliable = ms_ru * 1e-3;
+      info->seconds_final = ms_final ? *ms_final * 1e-3 : 0.0;
+    }
+    if (rc == QKX_ERR_NOT_CONVERGED && diverged)
+      set_error("mixed solve: %d right-hand side(s) diverged (FP64 true residual 1000x above its best) after %d "
+                "iterations; a larger reliable_delta keeps the sloppy recursion closer to the true residual",
+                diverged, iter);
+    else if (rc == QKX_ERR_NOT_CONVERGED)
+      set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
+    return rc;
   }
-  QKX_CUDA(cudaMemcpyAsync(sh, c->sc, sizeof(CgScalars), cudaMemcpyDeviceToHost, c->st));
-  if (device_loop) QKX_CUDA(cudaMemcpyAsync(hc, m->ctl, sizeof(MxCtl), cudaMemcpyDeviceToHost, c->st));
+};
+
+template <class P>
+static int invert_eo_mixed_t(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b,
+                             double2* const* x, qkx_solve_info* info) {
+  MixedSolve<P> s(c, sp, nrhs, b, x);
+  QKX_TRY(s.prepare(true));
+  MixedState* m = c->mixed;
+  QKX_CUDA(cudaEventRecord(c->t0, c->st));
+  QKX_TRY(s.setup());
+  QKX_CUDA(cudaEventRecord(m->ph[0], c->st));  // set-up done
+  if (s.device_loop) {
+    QKX_TRY(s.device_loop_launch());
+  } else {
+    QKX_TRY(s.host_loop());
+  }
+  QKX_CUDA(cudaEventRecord(m->ph[3], c->st));  // the final phase starts where the loop ended
+  QKX_TRY(s.final_phase());
   QKX_CUDA(cudaEventRecord(c->t1, c->st));
   QKX_CUDA(cudaEventSynchronize(c->t1));
-  QKX_CUDA(cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]));
-  if (device_loop) {
-    iter = hc->iter;
-    n_ru = hc->n_ru;
-    n_restart = hc->n_restart;
-    diverged = hc->diverged;
-    nact = hc->unconverged;
-    ms_ru = float(hc->ru_ns * 1e-6);
-    for (int i = 0; i < nrhs; i++) bnorm2[i] = hc->bnorm2[i];
-    counted(c, (int)(m->dgraph_k[0] + (long long)hc->n_outer * m->dgraph_k[1] + (long long)hc->iter * m->dgraph_k[2]));
-    if (hc->nan_iter > 0) {
-      set_error("mixed CG: r2 of right-hand side %d became non-finite at iteration %d", hc->nan_rhs, hc->nan_iter);
-      return QKX_ERR_NAN;
+  float ms = 0, ms_setup = 0, ms_final = 0;
+  cudaEventElapsedTime(&ms, c->t0, c->t1);
+  cudaEventElapsedTime(&ms_setup, c->t0, m->ph[0]);
+  cudaEventElapsedTime(&ms_final, m->ph[3], c->t1);
+  return s.finish(info, nullptr, &ms, &ms_setup, &ms_final);
+}
+
+// ---------------------------------------------------------------- many lattices in one graph launch
+// The jobs of qkx_invert_batch, grouped by context: the jobs of a context become one batch of
+// right-hand sides (each with its own twisted mass), and every context's solve -- set-up,
+// device-driven loop, final phase -- is one branch of a single CUDA graph.  One launch runs
+// all lattices; their kernels share the SMs as the branches go, so the small lattices' blocks
+// fill the gaps around the large one's.  Each branch ends with an event that dates it.
+struct BatchGroup {
+  qkx_ctx* c;
+  std::vector<int> jobs;        // job indices, in order
+  std::vector<int> first;       // first right-hand side of each job in the merged batch
+  std::vector<const double2*> b;
+  std::vector<double2*> x;
+  std::vector<double> mu;
+  qkx_solver_params p;
+  cudaEvent_t done = nullptr;
+};
+
+static double steady_seconds() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+template <class P>
+static int batch_graph_t(std::vector<BatchGroup>& groups, qkx_batch_job* jobs, const qkx_solver_params* sp,
+                         double t0) {
+  std::vector<std::unique_ptr<MixedSolve<P>>> solves;
+  for (BatchGroup& g : groups) {
+    solves.emplace_back(new MixedSolve<P>(g.c, &g.p, (int)g.b.size(), g.b.data(), g.x.data()));
+    QKX_TRY(solves.back()->prepare(true));
+    if (!solves.back()->device_loop) {
+      set_error("internal: the batch graph needs the device-driven loop");
+      return QKX_ERR_INVALID;
     }
   }
-  int rc = nact ? QKX_ERR_NOT_CONVERGED : QKX_OK;
-  double worst = 0.0;
-  int it = 0;
-  for (int i = 0; i < nrhs; i++) {
-    double rel = bnorm2[i] > 0 ? sqrt(sh->aux[i] / bnorm2[i]) : 0.0;
-    worst = std::max(worst, rel);
-    it = std::max(it, sh->iters[i]);
+  cudaStream_t master = groups[0].c->st;
+  cudaGraph_t top = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t start = nullptr;
+  QKX_CUDA(cudaGraphCreate(&top, 0));
+  int rc = QKX_OK;
+  for (size_t j = 0; j < groups.size() && rc == QKX_OK; j++) {
+    MixedSolve<P>& s = *solves[j];
+    BatchGroup& g = groups[j];
+    if (cudaEventCreate(&g.done) != cudaSuccess) {
+      set_error("batch: cudaEventCreate failed");
+      rc = QKX_ERR_CUDA;
+      break;
+    }
+    long long kt = 0, ko = 0, ki = 0;
+    rc = s.loop_graph(
+        top, &kt, &ko, &ki, [&]() { return s.setup(); },
+        [&]() -> int {
+          QKX_TRY(s.final_phase());
+          QKX_CUDA(cudaEventRecordWithFlags(g.done, g.c->st, cudaEventRecordExternal));
+          return QKX_OK;
+        });
+    s.kcount[0] = kt;
+    s.kcount[1] = ko;
+    s.kcount[2] = ki;
   }
-  if (rc == QKX_OK && worst > sp->tol) rc = QKX_ERR_NOT_CONVERGED;
-  if (info) {
-    info->iterations = it;
-    info->reliable_updates = n_ru;
-    info->restarts = n_restart;
-    info->converged = rc == QKX_OK;
-    info->true_residual = worst;
-    info->normal_residual = 0.0;
-    float ms = 0, ms_final = 0;
-    cudaEventElapsedTime(&ms, c->t0, c->t1);
-    cudaEventElapsedTime(&ms_final, m->ph[3], c->t1);
-    info->seconds = ms * 1e-3;
-    info->seconds_setup = ms_setup * 1e-3;
-    info->seconds_reliable = ms_ru * 1e-3;
-    info->seconds_final = ms_final * 1e-3;
+  if (rc == QKX_OK && cudaGraphInstantiate(&exec, top, 0) != cudaSuccess) {
+    set_error("batch: instantiating the graph failed: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = QKX_ERR_CUDA;
   }
-  if (rc == QKX_ERR_NOT_CONVERGED && diverged)
-    set_error("mixed solve: %d right-hand side(s) diverged (FP64 true residual 1000x above its best) after %d "
-              "iterations; a larger reliable_delta keeps the sloppy recursion closer to the true residual",
-              diverged, iter);
-  else if (rc == QKX_ERR_NOT_CONVERGED)
-    set_error("mixed solve: true residual %g above tol %g after %d iterations", worst, sp->tol, iter);
+  cudaGraphDestroy(top);
+  // work queued earlier on any context's stream comes first
+  for (size_t j = 1; j < groups.size() && rc == QKX_OK; j++) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess || cudaEventRecord(e, groups[j].c->st) != cudaSuccess ||
+        cudaStreamWaitEvent(master, e, 0) != cudaSuccess) {
+      set_error("batch: stream ordering failed");
+      rc = QKX_ERR_CUDA;
+    }
+    cudaEventDestroy(e);
+  }
+  const double t_host = steady_seconds() - t0;  // set-up and capture before the launch
+  if (rc == QKX_OK && (cudaEventCreate(&start) != cudaSuccess || cudaEventRecord(start, master) != cudaSuccess ||
+                       cudaGraphLaunch(exec, master) != cudaSuccess || cudaStreamSynchronize(master) != cudaSuccess)) {
+    set_error("batch: graph launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    rc = QKX_ERR_CUDA;
+  }
+  if (rc == QKX_OK) {
+    for (size_t j = 0; j < groups.size(); j++) {
+      BatchGroup& g = groups[j];
+      MixedSolve<P>& s = *solves[j];
+      float ms = 0;
+      cudaEventElapsedTime(&ms, start, g.done);
+      std::vector<double> rel(s.nrhs, 0.0);
+      qkx_solve_info info{};
+      const int src = s.finish(&info, rel.data(), &ms, nullptr, nullptr);
+      const char* msg = src == QKX_OK ? "" : qkx_last_error();
+      for (size_t q = 0; q < g.jobs.size(); q++) {
+        qkx_batch_job& jb = jobs[g.jobs[q]];
+        jb.info = info;
+        double worst = 0.0;
+        for (int r = g.first[q]; r < g.first[q] + jb.nrhs; r++) worst = std::max(worst, rel[r]);
+        jb.info.true_residual = worst;
+        jb.info.converged = src == QKX_OK || (src == QKX_ERR_NOT_CONVERGED && worst <= sp->tol) ? 1 : 0;
+        jb.status = src == QKX_ERR_NOT_CONVERGED && worst <= sp->tol ? QKX_OK : src;
+        jb.latency = t_host + ms * 1e-3;
+        snprintf(jb.message, sizeof jb.message, "%s", jb.status == QKX_OK ? "" : msg);
+      }
+    }
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (start) cudaEventDestroy(start);
+  for (BatchGroup& g : groups)
+    if (g.done) {
+      cudaEventDestroy(g.done);
+      g.done = nullptr;
+    }
   return rc;
+}
+
+// qkx_invert_batch for CG_EO_MIXED with graphs on: 0 = done (each job's status set), 1 = not
+// applicable (the caller runs the jobs one context per thread), < 0 = error.  Latencies count
+// from t0 (seconds of the steady clock).
+int invert_batch_graph(qkx_batch_job* jobs, int njobs, const qkx_solver_params* sp, double t0) {
+  if (sp->method != QKX_SOLVER_CG_EO_MIXED || sp->use_graphs == 0) return 1;
+  std::vector<BatchGroup> groups;
+  for (int i = 0; i < njobs; i++) {
+    qkx_ctx* c = jobs[i].ctx;
+    if (c->prof || (sp->sloppy_precision != QKX_PREC_DOUBLE && !c->compressible) || !c->have_gauge) return 1;
+    auto it = std::find_if(groups.begin(), groups.end(), [&](const BatchGroup& g) { return g.c == c; });
+    if (it == groups.end()) {
+      groups.emplace_back();
+      it = groups.end() - 1;
+      it->c = c;
+    }
+    it->jobs.push_back(i);
+    it->first.push_back((int)it->b.size());
+    for (int r = 0; r < jobs[i].nrhs; r++) {
+      it->b.push_back((const double2*)jobs[i].b_dev[r]);
+      it->x.push_back((double2*)jobs[i].x_dev[r]);
+      it->mu.push_back(jobs[i].mu ? jobs[i].mu[r] : c->p.mu);
+    }
+  }
+  int dev0 = groups[0].c->device;
+  for (BatchGroup& g : groups) {
+    if ((int)g.b.size() > MAX_RHS || g.c->device != dev0) return 1;
+    g.p = *sp;
+    g.p.mu = g.mu.data();
+  }
+  // the largest lattice's branch first
+  std::stable_sort(groups.begin(), groups.end(), [](const BatchGroup& a, const BatchGroup& b) { return a.c->V > b.c->V; });
+  QKX_CUDA(cudaSetDevice(dev0));
+  if (sp->sloppy_precision == QKX_PREC_HALF) return batch_graph_t<PHalf>(groups, jobs, sp, t0);
+  if (sp->sloppy_precision == QKX_PREC_SINGLE) return batch_graph_t<PSingle>(groups, jobs, sp, t0);
+  if (sp->sloppy_precision == QKX_PREC_DOUBLE) return batch_graph_t<PDouble>(groups, jobs, sp, t0);
+  set_error("invalid argument: sloppy_precision");
+  return QKX_ERR_INVALID;
 }
 
 // the captured graph holds gauge geometry: drop it when the gauge changes
@@ -1557,13 +1794,13 @@ int tune(qkx_ctx* c, int precision, int nrhs, int* nr, int* nt, double* ms) {
     }
   }
   if (precision == QKX_PREC_HALF) {
-    QKX_TRY(mixed_alloc<PHalf>(c, nrhs, false));
+    QKX_TRY(mixed_alloc<PHalf>(c, nrhs, true));
     rc = tune_tile<PHalf>(c, nrhs, &t, &best);
   } else if (precision == QKX_PREC_SINGLE) {
-    QKX_TRY(mixed_alloc<PSingle>(c, nrhs, false));
+    QKX_TRY(mixed_alloc<PSingle>(c, nrhs, true));
     rc = tune_tile<PSingle>(c, nrhs, &t, &best);
   } else if (precision == QKX_PREC_DOUBLE) {
-    QKX_TRY(mixed_alloc<PDouble>(c, nrhs, false));
+    QKX_TRY(mixed_alloc<PDouble>(c, nrhs, true));
     rc = tune_tile<PDouble>(c, nrhs, &t, &best);
   } else {
     set_error("invalid argument: precision");
