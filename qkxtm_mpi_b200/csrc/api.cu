@@ -2,13 +2,19 @@
 // the FP64 operators of the reference's qkxTM::Vector, the qkxTM BLAS and
 // the reference's CG (lib/solvers.cpp:16-81) on one B200.
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
+#include <stdint.h>
+
 #include <algorithm>
+#include <atomic>
+#include <mutex>
 
 #include "blas.cuh"
 #include "hop.cuh"
 #include "hop_c3.cuh"
+#include "hop_c3t.cuh"
 #include "layout.cuh"
 #include "qkx_ctx.cuh"
 #include "site_ops.cuh"
@@ -135,12 +141,99 @@ static double hop_bytes(size_t nout, double S, double G, bool both, bool extra_x
 // FP64 sites per block of the colour-split kernel (x 3 colour threads)
 constexpr int C3_NS = 64;
 
+// cuTensorMapEncodeTiled of the driver, looked up once (the library links the runtime only)
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                   const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static EncodeTiledFn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<EncodeTiledFn>(p);
+    cudaGetLastError();
+  });
+  return fn;
+}
+
+// A 2D TMA map over `rows` rows of Vh double2 (row stride Vh x 16 bytes) with boxes of `sites`
+// sites x `comps` rows, as FP64 elements (two per site and row).
+static bool map2d(CUtensorMap* m, const void* base, int Vh, int rows, int sites, int comps) {
+  const EncodeTiledFn f = encode_tiled();
+  if (!f || !base || ((uintptr_t)base & 15u)) return false;
+  const cuuint64_t dim[2] = {(cuuint64_t)2 * Vh, (cuuint64_t)rows};
+  const cuuint64_t stride[1] = {(cuuint64_t)Vh * 16};
+  const cuuint32_t box[2] = {(cuuint32_t)(2 * sites), (cuuint32_t)comps};
+  const cuuint32_t es[2] = {1, 1};
+  return f(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<void*>(base), dim, stride, box, es,
+           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// the TMA-tiled kernel for this launch, when the lattice and the fields allow it (else false)
+template <int B, bool DAG, int EPI>
+static bool launch_hop64_tiled(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A, const HopRes& Rz) {
+  const Geom& g = A.g;
+  if (!c->c3t || !c3t_supported(g, c->smem_optin)) return false;
+  if (A.nrhs > 1 && A.in.rs != (size_t)12 * g.Vh) return false;  // the batch must be [rhs][12][Vh]
+  const int W = g.L[0] / 2, Vh = g.Vh, rows = 12 * A.nrhs;
+  C3tMaps M;
+  memset(&M, 0, sizeof M);
+  for (int par = 0; par < 2; par++) {
+    const double2* base = par ? A.in.p1 : A.in.p0;
+    if (!base) continue;  // this input parity is not read by the launch
+    if (!map2d(&M.in4[par], base, Vh, rows, C3T_ROWS * W, 12) || !map2d(&M.in1[par], base, Vh, rows, W, 12))
+      return false;
+  }
+  const bool need0 = A.out_parity != 0, need1 = A.out_parity != 1;  // input parities: the other one
+  if ((need0 && !A.in.p0) || (need1 && !A.in.p1)) return false;
+  if (!map2d(&M.l4, A.gauge.p, Vh, 72, C3T_ROWS * W, 9) || !map2d(&M.l1, A.gauge.p, Vh, 72, W, 9) ||
+      !map2d(&M.l3, A.gauge.p, Vh, 72, (C3T_ROWS - 1) * W, 9))
+    return false;
+  // opt in once per device, to all the shared memory a block may have, so that concurrent
+  // contexts of different lattice sizes never lower one another's limit
+  const int smem = C3tLayout(W).bytes + 128;
+  static std::atomic<uint64_t> opted{0};
+  const uint64_t bit = 1ull << (c->device & 63);
+  if (!(opted.load() & bit)) {
+    if (cudaFuncSetAttribute(hop_c3t_kernel<B, DAG, EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             c->smem_optin) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    opted.fetch_or(bit);
+  }
+  A.nblk = c3t_blocks(g, A.out_parity);
+  hop_c3t_kernel<B, DAG, EPI><<<A.nblk, dim3(C3T_ROWS * W, 3), smem, c->st>>>(A, Rz, M, W, c->dstat);
+  counted(c);
+  return true;
+}
+
 // one FP64 18-real hop launch over A.nrhs right-hand sides (Rz: operands of EPI_XPAY_G5_RES)
 template <int B, bool DAG, int EPI>
-static void launch_hop64(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A, const HopRes& Rz = HopRes{}) {
+static int launch_hop64(qkx_ctx* c, HopArgs<SpinorF64, GaugeF64x18>& A, const HopRes& Rz = HopRes{}) {
+  if (launch_hop64_tiled<B, DAG, EPI>(c, A, Rz)) return QKX_OK;
   A.nblk = c3_blocks_per_rhs<C3_NS>(c->Vh, A.out_parity);
   hop_c3_kernel<C3_NS, SpinorF64, B, DAG, EPI><<<A.nblk * A.nrhs, dim3(C3_NS, 3), 0, c->st>>>(A, Rz);
   counted(c);
+  return QKX_OK;
+}
+
+int device_status(qkx_ctx* c) {
+  QKX_CUDA(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+  if (*c->hstat == 0) return QKX_OK;
+  const int code = *c->hstat;
+  *c->hstat = 0;
+  QKX_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(int), c->st));
+  QKX_CUDA(cudaStreamSynchronize(c->st));
+  set_error("a kernel's bounded wait for its shared-memory staging gave up (code %d): the results of the calls "
+            "since the last check are not valid",
+            code);
+  return QKX_ERR_CUDA;
 }
 
 template <int B, bool DAG, int EPI>
@@ -163,7 +256,7 @@ static int hop64_t(qkx_ctx* c, SpinorF64 in, SpinorF64 out, SpinorF64 x, bool x_
   A.active = nullptr;
   const int n = out_parity < 0 ? 2 * c->Vh : c->Vh;
   QKX_TRY(prof_begin(c));
-  launch_hop64<B, DAG, EPI>(c, A);
+  QKX_TRY((launch_hop64<B, DAG, EPI>(c, A)));
   QKX_CUDA(cudaGetLastError());
   bool extra = (EPI == EPI_XPAY || EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_TWINV) && x_distinct;
   return prof_end(c, hop_bytes(n, 192.0, 144.0, out_parity < 0, extra));
@@ -191,7 +284,7 @@ static int hop64_batch_t(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 out, Spin
   A.cvec = cvec;
   A.svec = svec;
   A.active = active;
-  launch_hop64<0, false, EPI>(c, A);
+  QKX_TRY((launch_hop64<0, false, EPI>(c, A)));
   QKX_CUDA(cudaGetLastError());
   if (nblk) *nblk = A.nblk;
   return QKX_OK;
@@ -215,8 +308,8 @@ int hop64_batch_res(qkx_ctx* c, int nrhs, SpinorF64 in, SpinorF64 x, SpinorF64 w
   A.cvec = cvec;
   A.svec = nullptr;
   A.active = active;
-  if (g5) launch_hop64<0, false, EPI_XPAY_G5_RES>(c, A, HopRes{w, res32});
-  else launch_hop64<0, false, EPI_XPAY_RES>(c, A, HopRes{w, res32});
+  if (g5) QKX_TRY((launch_hop64<0, false, EPI_XPAY_G5_RES>(c, A, HopRes{w, res32})));
+  else QKX_TRY((launch_hop64<0, false, EPI_XPAY_RES>(c, A, HopRes{w, res32})));
   QKX_CUDA(cudaGetLastError());
   if (nblk) *nblk = A.nblk;
   return QKX_OK;
@@ -521,7 +614,8 @@ int qkx_create(const qkx_params* p, int device, qkx_ctx** out) {
   }
   const size_t fbytes = sizeof(double2) * 12 * c->V;
   (void)fbytes;  // the staging buffer and the FP64 work fields are allocated on first use
-  c->npart = std::max(148 * 8, 2 * (int)((c->Vh + 31) / 32)) + 1;  // room for any hop block size >= 32
+  // room for any hop block size >= 32 and for the FP64 hop's row tiles
+  c->npart = std::max(std::max(148 * 8, 2 * (int)((c->Vh + 31) / 32)), c3t_blocks(c->geom, -1)) + 1;
   if (rc == QKX_OK && (e = cudaMalloc(&c->part, sizeof(double) * c->npart)) != cudaSuccess) fail(e, "partials");
   if (rc == QKX_OK && (e = cudaMalloc(&c->sc, sizeof(CgScalars))) != cudaSuccess) fail(e, "scalars");
   if (rc == QKX_OK && (e = cudaHostAlloc(&c->sc_h, sizeof(CgScalars), cudaHostAllocDefault)) != cudaSuccess)
@@ -529,6 +623,19 @@ int qkx_create(const qkx_params* p, int device, qkx_ctx** out) {
   if (rc == QKX_OK && (e = cudaMalloc(&c->dscal, sizeof(double) * 64)) != cudaSuccess) fail(e, "scalars");
   if (rc == QKX_OK && (e = cudaHostAlloc(&c->hscal, sizeof(double) * 64, cudaHostAllocDefault)) != cudaSuccess)
     fail(e, "pinned scalars");
+  if (rc == QKX_OK && (e = cudaMalloc(&c->dstat, sizeof(int))) != cudaSuccess) fail(e, "status word");
+  if (rc == QKX_OK && (e = cudaMemset(c->dstat, 0, sizeof(int))) != cudaSuccess) fail(e, "status word");
+  if (rc == QKX_OK && (e = cudaHostAlloc(&c->hstat, sizeof(int), cudaHostAllocDefault)) != cudaSuccess)
+    fail(e, "pinned status word");
+  if (rc == QKX_OK &&
+      (e = cudaDeviceGetAttribute(&c->smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device)) != cudaSuccess)
+    fail(e, "device attribute");
+  {
+    // QKX_FP64_TILED=1 puts the FP64 hop on the TMA row tiles (hop_c3t.cuh) where the lattice
+    // allows them; the direct kernel is the default, as it is the faster of the two on B200
+    const char* v = getenv("QKX_FP64_TILED");
+    c->c3t = (v && v[0] == '1') ? 1 : 0;
+  }
   if (rc == QKX_OK && (e = cudaEventCreate(&c->t0)) != cudaSuccess) fail(e, "event");
   if (rc == QKX_OK && (e = cudaEventCreate(&c->t1)) != cudaSuccess) fail(e, "event");
   if (rc != QKX_OK) {
@@ -557,6 +664,8 @@ void qkx_destroy(qkx_ctx* c) {
   cudaFree(c->U18hc);
   cudaFree(c->Usm);
   cudaFree(c->stage);
+  cudaFree(c->dstat);
+  if (c->hstat) cudaFreeHost(c->hstat);
   for (int i = 0; i < qkx_ctx::NW; i++) cudaFree(c->w[i]);
   cudaFree(c->part);
   cudaFree(c->sc);
@@ -680,7 +789,7 @@ int qkx_apply(qkx_ctx* c, int op, const double* in_host, double* out_host) {
   QKX_TRY(run_op(c, op, c->w[0], c->w[1]));
   QKX_TRY(download_spinor(c, c->w[1], out_host));
   QKX_CUDA(cudaStreamSynchronize(c->st));
-  return QKX_OK;
+  return device_status(c);
 }
 
 int qkx_spinor_upload(qkx_ctx* c, const double* host, double* dev) {
@@ -800,6 +909,7 @@ int qkx_cg_dev(qkx_ctx* c, const double* in_dev, double* x_dev, qkx_solve_info* 
   int rc = cg_fp64_loop(c, x, r, p, Ap, tmp, stop, c->p.maxIter, &k, &r2);
   QKX_CUDA(cudaEventRecord(c->t1, c->st));
   QKX_CUDA(cudaEventSynchronize(c->t1));
+  QKX_TRY(device_status(c));
   if (info) {
     memset(info, 0, sizeof *info);
     info->iterations = k;
@@ -918,10 +1028,13 @@ int qkx_invert_dev(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
   if (info) memset(info, 0, sizeof *info);
   const double2* const* b = (const double2* const*)b_dev;
   double2* const* x = (double2* const*)x_dev;
-  if (sp->method == QKX_SOLVER_CG_FP64) return invert_cg_fp64(c, sp, nrhs, b, x, info);
-  if (sp->method == QKX_SOLVER_CG_EO_MIXED) return invert_eo_mixed(c, sp, nrhs, b, x, info);
-  if (sp->method == QKX_SOLVER_GCR_PTC) return invert_gcr_ptc(c, sp, nrhs, b, x, info);
-  return invalid("solver method");
+  int rc;
+  if (sp->method == QKX_SOLVER_CG_FP64) rc = invert_cg_fp64(c, sp, nrhs, b, x, info);
+  else if (sp->method == QKX_SOLVER_CG_EO_MIXED) rc = invert_eo_mixed(c, sp, nrhs, b, x, info);
+  else if (sp->method == QKX_SOLVER_GCR_PTC) rc = invert_gcr_ptc(c, sp, nrhs, b, x, info);
+  else return invalid("solver method");
+  const int st = device_status(c);  // a bounded device wait that gave up voids the solution
+  return st != QKX_OK ? st : rc;
 }
 
 int qkx_invert(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double* const* b_host,

@@ -80,6 +80,65 @@ __device__ __forceinline__ Spin4<double> twist_inv4(const Spin4<double>& v, doub
   return o;
 }
 
+// The fused epilogue of one colour thread (colour a of output site cb, parity par, right-hand
+// side rhs) from its accumulated hopping term; stores the output (or, for the residual
+// epilogues, the FP32 residual) and returns this thread's share of |output|^2 (|residual|^2).
+template <class SP, int B, int EPI>
+__device__ __forceinline__ double c3_epilogue(const HopArgs<SP, GaugeF64x18>& A, const HopRes& Rz, int rhs, int par,
+                                              int cb, int a, const Spin4<double>& acc) {
+  const double c = A.c * (A.cvec ? A.cvec[rhs] : 1.0);
+  const double sc = A.s * (A.svec ? A.svec[rhs] : 1.0);
+  const int Vh = A.g.Vh;
+  double nrm = 0.0;
+  Spin4<double> o;
+  if constexpr (EPI == EPI_PLAIN) {
+    o = acc;
+  } else if constexpr (EPI == EPI_TWIST_INV) {
+    o = twist_inv4<B>(acc, c, sc);
+  } else {
+    const SP xs = A.x.shift(rhs);
+    const double2* xb = (par ? xs.p1 : xs.p0) + cb;
+    Spin4<double> v;
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) v.s[sp] = ldc(xb + (size_t)(sp * 3 + a) * Vh);
+    if constexpr (EPI == EPI_XPAY_TWINV) {
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) v.s[sp] = A.a * acc.s[sp] + v.s[sp];
+      o = twist_inv4<B>(v, c, sc);
+    } else {
+      const Spin4<double> g5v = gamma5_4<B>(v);
+#pragma unroll
+      for (int sp = 0; sp < 4; sp++) o.s[sp] = A.a * acc.s[sp] + (v.s[sp] + c * phase<1>(g5v.s[sp]));
+      if constexpr (EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_RES) o = gamma5_4<B>(o);
+    }
+  }
+  if constexpr (EPI == EPI_XPAY_G5_RES || EPI == EPI_XPAY_RES) {
+    // res = w - o in FP64 and its norm; stored (when a target is given) as FP32, complex
+    // k = sp*3 + a in half k%2 of float4 word k/2
+    const SpinorF64 ws = Rz.w.shift(rhs);
+    const double2* wb = (par ? ws.p1 : ws.p0) + cb;
+    const SpinorF32 rs = Rz.res32.shift(rhs);
+    float4* rq = par ? rs.p1 : rs.p0;
+    float2* rb = rq ? reinterpret_cast<float2*>(rq + cb) : nullptr;
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) {
+      const Cx<double> z = ldc(wb + (size_t)(sp * 3 + a) * Vh) - o.s[sp];
+      nrm += z.re * z.re + z.im * z.im;
+      const int k = sp * 3 + a;
+      if (rb) rb[2 * (size_t)(k >> 1) * Vh + (k & 1)] = make_float2(float(z.re), float(z.im));
+    }
+  } else {
+    const SP os = A.out.shift(rhs);
+    double2* ob = (par ? os.p1 : os.p0) + cb;
+#pragma unroll
+    for (int sp = 0; sp < 4; sp++) {
+      ob[(size_t)(sp * 3 + a) * Vh] = make_double2(o.s[sp].re, o.s[sp].im);
+      nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
+    }
+  }
+  return nrm;
+}
+
 template <int NS, class SP, int B, bool DAG, int EPI>
 __global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18> A, HopRes Rz) {
   const int rhs = blockIdx.x % A.nrhs;
@@ -112,56 +171,7 @@ __global__ void __launch_bounds__(NS * 3) hop_c3_kernel(HopArgs<SP, GaugeF64x18>
     hop_dir_c3<SP, B, DAG, 1>(in, A.gauge, A.g, par, cb, x, s, L0, a, acc);
     hop_dir_c3<SP, B, DAG, 2>(in, A.gauge, A.g, par, cb, x, s, L01, a, acc);
     hop_dir_c3<SP, B, DAG, 3>(in, A.gauge, A.g, par, cb, x, s, L012, a, acc);
-
-    const double c = A.c * (A.cvec ? A.cvec[rhs] : 1.0);
-    const double sc = A.s * (A.svec ? A.svec[rhs] : 1.0);
-    const int Vh = A.g.Vh;
-    Spin4<double> o;
-    if constexpr (EPI == EPI_PLAIN) {
-      o = acc;
-    } else if constexpr (EPI == EPI_TWIST_INV) {
-      o = twist_inv4<B>(acc, c, sc);
-    } else {
-      const SP xs = A.x.shift(rhs);
-      const double2* xb = (par ? xs.p1 : xs.p0) + cb;
-      Spin4<double> v;
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) v.s[sp] = ldc(xb + (size_t)(sp * 3 + a) * Vh);
-      if constexpr (EPI == EPI_XPAY_TWINV) {
-#pragma unroll
-        for (int sp = 0; sp < 4; sp++) v.s[sp] = A.a * acc.s[sp] + v.s[sp];
-        o = twist_inv4<B>(v, c, sc);
-      } else {
-        const Spin4<double> g5v = gamma5_4<B>(v);
-#pragma unroll
-        for (int sp = 0; sp < 4; sp++) o.s[sp] = A.a * acc.s[sp] + (v.s[sp] + c * phase<1>(g5v.s[sp]));
-        if constexpr (EPI == EPI_XPAY_G5 || EPI == EPI_XPAY_G5_RES) o = gamma5_4<B>(o);
-      }
-    }
-    if constexpr (EPI == EPI_XPAY_G5_RES || EPI == EPI_XPAY_RES) {
-      // res = w - o in FP64 and its norm; stored (when a target is given) as FP32, complex
-      // k = sp*3 + a in half k%2 of float4 word k/2
-      const SpinorF64 ws = Rz.w.shift(rhs);
-      const double2* wb = (par ? ws.p1 : ws.p0) + cb;
-      const SpinorF32 rs = Rz.res32.shift(rhs);
-      float4* rq = par ? rs.p1 : rs.p0;
-      float2* rb = rq ? reinterpret_cast<float2*>(rq + cb) : nullptr;
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        const Cx<double> z = ldc(wb + (size_t)(sp * 3 + a) * Vh) - o.s[sp];
-        nrm += z.re * z.re + z.im * z.im;
-        const int k = sp * 3 + a;
-        if (rb) rb[2 * (size_t)(k >> 1) * Vh + (k & 1)] = make_float2(float(z.re), float(z.im));
-      }
-    } else {
-      const SP os = A.out.shift(rhs);
-      double2* ob = (par ? os.p1 : os.p0) + cb;
-#pragma unroll
-      for (int sp = 0; sp < 4; sp++) {
-        ob[(size_t)(sp * 3 + a) * Vh] = make_double2(o.s[sp].re, o.s[sp].im);
-        nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
-      }
-    }
+    nrm = c3_epilogue<SP, B, EPI>(A, Rz, rhs, par, cb, a, acc);
   }
   if (slot) {
     __shared__ double red[(NS * 3 + 31) / 32];

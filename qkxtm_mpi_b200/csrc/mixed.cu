@@ -39,6 +39,7 @@
 #include "hop.cuh"
 #include "hop_mrhs.cuh"
 #include "hop_pair.cuh"
+#include "hop_c3t.cuh"
 #include "qkx_ctx.cuh"
 #include "site_ops.cuh"
 
@@ -629,8 +630,10 @@ static int mixed_alloc(qkx_ctx* c, int R, bool solver) {
     if (rc == QKX_OK && !f->d) rc = bfield_alloc<typename P::SP>(*f, m->R, Vh);
   if (rc == QKX_OK && !m->cvec && cudaMalloc(&m->cvec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
   if (rc == QKX_OK && !m->svec && cudaMalloc(&m->svec, sizeof(double) * MAX_RHS) != cudaSuccess) rc = QKX_ERR_NOMEM;
-  // partials: the smallest hop block (64 threads) over both parities, or the streaming grid
-  const size_t nblk = (size_t)hop_blocks_per_rhs<64>(Vh, -1) + MX_GRID;
+  // partials: the smallest hop block (64 threads) or the FP64 hop's row tiles (whichever is more)
+  // over both parities, plus the streaming grid
+  const size_t nblk =
+      (size_t)std::max(hop_blocks_per_rhs<64>(Vh, -1), c3t_blocks(c->geom, -1)) + MX_GRID;
   if (rc == QKX_OK && !m->part && cudaMalloc(&m->part, sizeof(double) * (size_t)m->R * nblk) != cudaSuccess)
     rc = QKX_ERR_NOMEM;
   if (solver) {
@@ -1591,7 +1594,9 @@ static int batch_graph_t(std::vector<BatchGroup>& groups, qkx_batch_job* jobs, c
       cudaEventElapsedTime(&ms, start, g.done);
       std::vector<double> rel(s.nrhs, 0.0);
       qkx_solve_info info{};
-      const int src = s.finish(&info, rel.data(), &ms, nullptr, nullptr);
+      int src = s.finish(&info, rel.data(), &ms, nullptr, nullptr);
+      const int st = device_status(g.c);  // a bounded device wait that gave up voids the solution
+      if (st != QKX_OK) src = st;
       const char* msg = src == QKX_OK ? "" : qkx_last_error();
       for (size_t q = 0; q < g.jobs.size(); q++) {
         qkx_batch_job& jb = jobs[g.jobs[q]];

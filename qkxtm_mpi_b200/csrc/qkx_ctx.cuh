@@ -69,6 +69,10 @@ struct qkx_ctx {
   qkx::CgScalars* sc_h = nullptr;  // pinned host mirror
   double* dscal = nullptr;         // device scratch scalars [64]
   double* hscal = nullptr;         // pinned host scalars [64]
+  int* dstat = nullptr;            // device status word: non-zero after a bounded device wait gave up
+  int* hstat = nullptr;            // pinned host copy
+  int smem_optin = 0;              // shared memory a block may opt in to on this device
+  int c3t = 0;                     // the TMA-tiled FP64 hop where the lattice allows it (opt-in)
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   // profiling of the hopping kernels
   int prof = 0;
@@ -159,6 +163,10 @@ int set_tile(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind);
 int tune_table(qkx_ctx* c, int precision, int nrhs, int max, int* count, int* nr, int* nt, int* kind, double* ms);
 int sloppy_normal(qkx_ctx* c, int precision, int nrhs, int nr, int nt, int kind, const double* const* in_host,
                   double* const* out_host);
+
+// the device status word: QKX_ERR_CUDA (and the word cleared) if a kernel's bounded wait gave
+// up since the last check; synchronizes the context's stream
+int device_status(qkx_ctx* c);
 
 // lazy buffers and context-level helpers (api.cu)
 int ensure_stage(qkx_ctx* c);

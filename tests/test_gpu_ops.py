@@ -215,3 +215,55 @@ def test_errors_are_status_codes(qkx, oracle):
         assert qkx.lib().qkx_apply(lat.ctx, 999, psi.ctypes.data, out.ctypes.data) == qkx.ERR_INVALID
         assert qkx.lib().qkx_set_params(lat.ctx, C.byref(qkx.LatticeInfo(L=(4, 4, 4, 8)).to_c())) == \
             qkx.ERR_INVALID
+
+
+# Row widths W = L0/2 from 1 to 16 (12W threads a block: 12, 48, 72, 144 leave the last warp
+# partial), y extents that are multiples of the four-row tile, extents of 2 in z and t (the
+# +-z and +-t planes coincide)
+TILED = [(2, 4, 2, 2), (4, 4, 4, 8), (6, 4, 2, 10), (8, 8, 8, 16), (12, 4, 2, 4), (16, 4, 4, 4),
+         (24, 4, 2, 2), (32, 4, 2, 2)]
+
+
+@pytest.mark.parametrize("L", TILED)
+def test_tiled_fp64_hop_matches_direct_kernel(qkx, oracle, monkeypatch, L):
+    """The FP64 hop on TMA-staged row tiles (QKX_FP64_TILED=1, where L0 <= 32 and Ly % 4 == 0)
+    against the direct kernel (the default) and the oracle, every operator."""
+    U, psi = _inputs(oracle, L, 0.3, 300 + L[0], 400 + L[3])
+    monkeypatch.setenv("QKX_FP64_TILED", "0")
+    direct = qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004, twistSign=1))
+    monkeypatch.setenv("QKX_FP64_TILED", "1")
+    tiled = qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004, twistSign=1))
+    try:
+        for lat in (direct, tiled):
+            lat.load_gauge(U, qkx.LINKS_AS_GIVEN)
+        for op in oracle.REF_OPS:
+            a, b = tiled.apply(op, psi), direct.apply(op, psi)
+            assert rel(a, b) <= 1e-15, (L, op, rel(a, b))
+            assert rel(a, oracle.apply(op, L, U, psi, 0.1615, 0.004, 1)) < TOL, (L, op)
+    finally:
+        direct.close()
+        tiled.close()
+
+
+@pytest.mark.parametrize("prec", ["half", "double"])
+def test_tiled_fp64_hop_in_the_mixed_solver(qkx, oracle, monkeypatch, prec):
+    """Batched right-hand sides through the reliable updates and the final reconstruction
+    (FP64 hops with residual and norm epilogues): tiled and direct kernels give the same
+    solutions to the solver's accuracy, each to 1e-10 in the true residual."""
+    L = (16, 8, 4, 8)
+    U = oracle.apply_bc(L, oracle.gauge_random(L, 0.3, 777), -1)
+    bs = [oracle.spinor_gaussian(L, 30 + i) for i in range(3)]
+    p = {"half": qkx.PREC_HALF, "double": qkx.PREC_DOUBLE}[prec]
+    out = {}
+    for mode in ("0", "1"):
+        monkeypatch.setenv("QKX_FP64_TILED", mode)
+        with qkx.Lattice(qkx.LatticeInfo(L=L, kappa=0.1615, mu=0.004, twistSign=1)) as lat:
+            lat.load_gauge(U)
+            xs, info = lat.invert(bs, method=qkx.SOLVER_CG_EO_MIXED, precision=p, tol=1e-10)
+        assert info.converged == 1
+        for x, b in zip(xs, bs):
+            r = b - oracle.apply("tm", L, U, x, 0.1615, 0.004, 1)
+            assert np.sqrt(np.sum(r * r) / np.sum(b * b)) <= 1e-10
+        out[mode] = xs
+    for a, b in zip(out["0"], out["1"]):
+        assert rel(a, b) < 1e-8
