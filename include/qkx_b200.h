@@ -224,9 +224,11 @@ QKX_API int qkx_cg_dev(qkx_ctx* ctx, const double* in_dev, double* x_dev, qkx_so
 /* Solver methods for qkx_invert. */
 #define QKX_SOLVER_CG_FP64 0        /* plain FP64 CG on M^+M, full lattice (the reference's method) */
 #define QKX_SOLVER_CG_EO_MIXED 1    /* even-odd Schur CG, sloppy spinors/links, FP64 reliable updates */
-#define QKX_SOLVER_GCR_PTC 2        /* flexible GCR(16) on M in FP32 with the learned preconditioner
-                                       (sp->preconditioner; NULL = none), FP64 defect correction,
-                                       and CG_EO_MIXED as the fallback */
+#define QKX_SOLVER_GCR_PTC 2        /* the learned solver: all right-hand sides in one batch on the
+                                       even-odd Schur system, flexible CG on its normal equations in
+                                       FP32 preconditioned by K K^+ (K the network sp->preconditioner
+                                       on the even sites; NULL = none), FP64 defect correction, and
+                                       CG_EO_MIXED as the fallback */
 
 #define QKX_PREC_DOUBLE 0
 #define QKX_PREC_SINGLE 1
@@ -491,9 +493,12 @@ typedef struct qkx_ptc_params {
 } qkx_ptc_params;
 
 typedef struct qkx_ptc_train_params {
-  int n_solves;            /* (residual, error) pairs from as many mixed-precision CG solves of
-                              Gaussian sources, r = b and e = M^-1 b, plus as many pairs r = M v,
-                              e = v for Gaussian v (the short-distance part of M^-1) */
+  int n_solves;            /* (residual, error) pairs on the even-odd Schur system Mh x_e = b^_e
+                              that QKX_SOLVER_GCR_PTC preconditions: from as many mixed-precision
+                              CG solves of Gaussian sources b, r = b^_e and e = x_e, plus as many
+                              pairs r = Mh v_e, e = v_e for Gaussian v (the short-distance part of
+                              Mh^-1); inputs are zero on the odd sites, the loss counts the even
+                              sites */
   int steps;               /* Adam steps, one pair each, pairs in a seeded shuffled order */
   double lr;               /* peak learning rate (cosine decay to lr/20) */
   double solve_tol;        /* true-residual tolerance of the data solves */
@@ -501,7 +506,8 @@ typedef struct qkx_ptc_train_params {
 } qkx_ptc_train_params;
 
 typedef struct qkx_ptc_train_info {
-  double loss_initial;     /* mean |N(r) - e|^2 / |e|^2 over up to 4 pairs of each kind, before */
+  double loss_initial;     /* mean |N(r) - e|^2 / |e|^2 (even sites) over up to 4 pairs of each
+                              kind, before */
   double loss_final;       /* the same after training */
   double seconds_data;     /* device time of the data solves */
   double seconds_train;    /* device time of the training steps */

@@ -46,6 +46,9 @@ def _worker(args):
     return time.perf_counter() - t0
 
 
+_ITERS_CACHE: dict = {}
+
+
 def iterations_to_converge(L, kappa, mu, eps, seed, tol=1e-10) -> tuple[int, float]:
     """Iterations the reference's CG recurrence (lib/solvers.cpp:16-81) needs on
     a lattice small enough to solve quickly, same parameters, point source, to
@@ -54,7 +57,15 @@ def iterations_to_converge(L, kappa, mu, eps, seed, tol=1e-10) -> tuple[int, flo
     The reference stops on the normal-equation residual r2 <= tol^2 |M^+ b|^2,
     which leaves the true residual somewhat above tol; the stop is tightened
     (and the solve repeated from zero) until the true residual meets tol, as the
-    GPU's plain FP64 CG does.  Returns (iterations, true residual reached)."""
+    GPU's plain FP64 CG does.  Returns (iterations, true residual reached); the
+    result is cached per parameter set for the life of the process."""
+    key = (tuple(L), kappa, mu, eps, seed, tol)
+    if key not in _ITERS_CACHE:
+        _ITERS_CACHE[key] = _iterations_to_converge(L, kappa, mu, eps, seed, tol)
+    return _ITERS_CACHE[key]
+
+
+def _iterations_to_converge(L, kappa, mu, eps, seed, tol):
     U = O.apply_bc(L, O.gauge_random(L, eps, seed), -1)
     b = O.spinor_point(L, (0, 0, 0, 0), 0, 0)
     Mdb = O.apply("tm_dag", L, U, b, kappa, mu, 1)
@@ -69,9 +80,24 @@ def iterations_to_converge(L, kappa, mu, eps, seed, tol=1e-10) -> tuple[int, flo
     return k, true
 
 
+def write_links(links: np.ndarray) -> str:
+    """The links as a raw FP64 file for the worker processes (in /dev/shm when it has
+    room); the caller removes it."""
+    import shutil
+    tmpdir = tempfile.gettempdir()
+    if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > 2 * links.nbytes:
+        tmpdir = "/dev/shm"
+    fd, path = tempfile.mkstemp(prefix="qkx_links_", suffix=".f64", dir=tmpdir)
+    os.close(fd)
+    links.astype(np.float64).tofile(path)
+    return path
+
+
 def run(L, kappa, mu, eps, seed, n_sources=12, n_iter=1, procs=None, iters_full=None,
-        links: np.ndarray | None = None, timeout: float = 900.0) -> dict:
+        links: np.ndarray | None = None, timeout: float = 900.0, links_path: str | None = None) -> dict:
     """Time the CPU hot path and project it to solving n_sources point sources.
+    links_path: the links already written by write_links (kept), else they are
+    written for this call and removed after it.
 
     Returns {"value": seconds for the whole job, "per_iter_s", "cores", "kind",
     "sample", "iters_full"}."""
@@ -79,16 +105,14 @@ def run(L, kappa, mu, eps, seed, n_sources=12, n_iter=1, procs=None, iters_full=
     kind = "reference" if O.ref_available() else "port"
     ncpu = os.cpu_count() or 1
     P = max(1, min(n_sources, ncpu if procs is None else procs))
-    if links is None:
-        links = O.apply_bc(L, O.gauge_random(L, eps, seed), -1)
-    import shutil
-    tmpdir = tempfile.gettempdir()
-    if os.path.isdir("/dev/shm") and shutil.disk_usage("/dev/shm").free > 2 * links.nbytes:
-        tmpdir = "/dev/shm"
-    fd, path = tempfile.mkstemp(prefix="qkx_links_", suffix=".f64", dir=tmpdir)
-    os.close(fd)
+    own = links_path is None
+    if own:
+        if links is None:
+            links = O.apply_bc(L, O.gauge_random(L, eps, seed), -1)
+        path = write_links(links)
+    else:
+        path = links_path
     try:
-        links.astype(np.float64).tofile(path)
         root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
         env = dict(os.environ, PYTHONPATH=root + os.pathsep + os.environ.get("PYTHONPATH", ""))
         t0 = time.perf_counter()
@@ -111,7 +135,8 @@ def run(L, kappa, mu, eps, seed, n_sources=12, n_iter=1, procs=None, iters_full=
             times.append(float(out.strip().splitlines()[-1]))
         wall = time.perf_counter() - t0
     finally:
-        os.unlink(path)
+        if own:
+            os.unlink(path)
     per_iter = float(np.median(times)) / n_iter
     if iters_full is None:
         small = (8, 8, 8, 16)

@@ -106,6 +106,7 @@ def lib():
         L.orc_ptc_forward.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
         L.orc_ptc_loss_grad.argtypes = [_ip, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
         L.orc_ptc_loss_grad.restype = C.c_double
+        L.orc_ptc_act_bf16.argtypes = [C.c_int]
     return _lib
 
 
@@ -369,22 +370,32 @@ def ptc_nweights(ch) -> int:
     return int(lib().orc_ptc_nweights(len(ch) - 1, (C.c_int * len(ch))(*ch)))
 
 
-def ptc_forward(L, U, ch, W, x) -> np.ndarray:
-    """N(x) for x [V, ch[0], 3, 2]; W complex weights as float64 [nweights, 2]."""
+def ptc_forward(L, U, ch, W, x, bf16=False) -> np.ndarray:
+    """N(x) for x [V, ch[0], 3, 2]; W complex weights as float64 [nweights, 2].  bf16: the
+    hidden activations rounded to BF16 as the GPU stores them (arithmetic FP64)."""
     V = volume(L)
     out = np.empty((V, ch[-1], 3, 2))
-    lib().orc_ptc_forward(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1, (C.c_int * len(ch))(*ch),
-                          _ptr(np.ascontiguousarray(W)), _ptr(np.ascontiguousarray(x)), _ptr(out), None)
+    lib().orc_ptc_act_bf16(1 if bf16 else 0)
+    try:
+        lib().orc_ptc_forward(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1, (C.c_int * len(ch))(*ch),
+                              _ptr(np.ascontiguousarray(W)), _ptr(np.ascontiguousarray(x)), _ptr(out), None)
+    finally:
+        lib().orc_ptc_act_bf16(0)
     return out
 
 
-def ptc_loss_grad(L, U, ch, W, r, e, grad=True):
-    """(|N(r) - e|^2 / |e|^2, dL/dW^* as [nweights, 2] or None)."""
+def ptc_loss_grad(L, U, ch, W, r, e, grad=True, bf16=False):
+    """(|N(r) - e|^2 / |e|^2, dL/dW^* as [nweights, 2] or None); bf16 as in ptc_forward, for
+    the activation gradients between layers too."""
     g = np.zeros_like(W) if grad else None
-    loss = lib().orc_ptc_loss_grad(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1,
-                                   (C.c_int * len(ch))(*ch), _ptr(np.ascontiguousarray(W)),
-                                   _ptr(np.ascontiguousarray(r)), _ptr(np.ascontiguousarray(e)),
-                                   _ptr(g) if grad else None)
+    lib().orc_ptc_act_bf16(1 if bf16 else 0)
+    try:
+        loss = lib().orc_ptc_loss_grad(_L(L), _ptr(np.ascontiguousarray(U)), len(ch) - 1,
+                                       (C.c_int * len(ch))(*ch), _ptr(np.ascontiguousarray(W)),
+                                       _ptr(np.ascontiguousarray(r)), _ptr(np.ascontiguousarray(e)),
+                                       _ptr(g) if grad else None)
+    finally:
+        lib().orc_ptc_act_bf16(0)
     return loss, g
 
 

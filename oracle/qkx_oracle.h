@@ -111,6 +111,8 @@ void orc_ptc_forward(const int L[4], const double* U, int nlayers, const int* ch
                      const double* in, double* out, double* acts);
 double orc_ptc_loss_grad(const int L[4], const double* U, int nlayers, const int* ch, const double* W,
                          const double* r, const double* e, double* grad);
+/* 1: hidden activations and activation gradients stored as BF16 (as on the GPU); 0: FP64 */
+void orc_ptc_act_bf16(int on);
 
 #ifdef __cplusplus
 }

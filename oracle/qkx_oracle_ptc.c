@@ -28,10 +28,35 @@
 #include "qkx_oracle.h"
 
 #include <complex.h>
+#include <stdint.h>
 #include <stdlib.h>
 #include <string.h>
 
 typedef double _Complex cplx;
+
+/* Optional BF16 storage of the activations between layers, as the GPU keeps them:
+ * when on, every hidden activation (the output of layers 0..nlayers-2) and every
+ * activation gradient between layers is rounded to BF16 (round to nearest even,
+ * from its FP32 value) after it is computed; the arithmetic stays FP64. */
+static int act_bf16 = 0;
+void orc_ptc_act_bf16(int on) { act_bf16 = on; }
+
+static double bf16_round(double v) {
+  float f = (float)v;
+  uint32_t u;
+  memcpy(&u, &f, 4);
+  if ((u & 0x7f800000u) != 0x7f800000u) { /* finite: add half an ulp (ties to even), truncate */
+    u += 0x7fffu + ((u >> 16) & 1u);
+    u &= 0xffff0000u;
+  }
+  memcpy(&f, &u, 4);
+  return (double)f;
+}
+
+static void round_field(cplx* a, long n) {
+  if (!act_bf16) return;
+  for (long i = 0; i < n; i++) a[i] = bf16_round(creal(a[i])) + I * bf16_round(cimag(a[i]));
+}
 
 static long nbr(const int L[4], long s, int mu, int d) {
   int c[4];
@@ -110,6 +135,7 @@ void orc_ptc_forward(const int L[4], const double* Ud, int nlayers, const int* c
       store += V * ch[l] * 3;
     }
     layer(L, U, W, ch[l], ch[l + 1], a, b);
+    if (l < nlayers - 1) round_field(b, V * ch[l + 1] * 3);
     W += weights_per_layer(ch, l);
     cplx* t = a;
     a = b;
@@ -183,6 +209,7 @@ double orc_ptc_loss_grad(const int L[4], const double* Ud, int nlayers, const in
           }
         }
       }
+      round_field(h, V * Ci * 3);
       cplx* t = g;
       g = h;
       h = t;

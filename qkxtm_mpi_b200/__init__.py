@@ -26,6 +26,7 @@ missing or fails.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 import os
 from dataclasses import dataclass, field
 from typing import Sequence
@@ -318,9 +319,12 @@ class Lattice:
         p = info.to_c()
         check(lib().qkx_create(C.byref(p), device, C.byref(ctx)))
         self.ctx = ctx
+        self._owned = weakref.WeakSet()  # networks on this context, closed before it
 
     def close(self):
         if getattr(self, "ctx", None):
+            for o in list(getattr(self, "_owned", ())):
+                o.close()
             lib().qkx_destroy(self.ctx)
             self.ctx = None
 
@@ -677,11 +681,13 @@ class Ptc:
         self.ptr = _vp()
         check(lib().qkx_ptc_create(lat.ctx, C.byref(p), C.byref(self.ptr)))
         self.nw = int(lib().qkx_ptc_num_weights(self.ptr))
+        lat._owned.add(self)
 
     def close(self):
-        if getattr(self, "ptr", None) and self.ptr.value:
+        # a network lives on its lattice's context: the lattice closes it first when it closes
+        if getattr(self, "ptr", None) and self.ptr.value and getattr(self.lat, "ctx", None):
             lib().qkx_ptc_destroy(self.ptr)
-            self.ptr = _vp()
+        self.ptr = _vp()
 
     def __del__(self):
         try:

@@ -8,13 +8,28 @@
 // SU(3), boundary sign applied from the t coordinate), so the network
 // commutes with gauge transformations as M^-1 does.  No reference counterpart.
 //
-// Activation layout: even-odd, [parity][3C/2][Vh] float4, complex number
-// k = c*3 + colour in word k/2, so channels c, c+1 fill three float4 words.
-// For C = 4 this is exactly the FP32 spinor layout (SpinorF32), which lets the
-// solver's fields be the network's input and output.
+// Why the channels are colour vectors.  A gauge transformation acts on the
+// colour index of every site.  A layer whose weights mixed colour components
+// (a 12 -> 16 complex map of a site's spin-colour numbers) would not commute
+// with it; the weights must act on a channel index and leave colour to the
+// transports.  A spin-colour spinor is therefore 4 channels of colour vectors,
+// and a hidden width of 16 channels is 16 colour vectors (48 complex numbers a
+// site): the gauge-covariant form of a 12 -> 16 -> 16 -> 12 complex network is
+// 4 -> 16 -> 16 -> 4 here.
+//
+// Activation fields.  Channel c, colour b of a site is complex number
+// k = c*3 + b; the four channels of group q = c/4 are 12 complex numbers in
+// three 16-byte words (word k'/4, slot k'%4 for k' = k - 12q).
+//   BF16 (hidden activations and their gradients): per parity [C/4][3][Vh]
+//         uint4, each complex one __nv_bfloat162 (re, im) -- 48 B a site and
+//         group, half of FP32;
+//   FP32 (network input and output, C = 4): the solver's FP32 spinor, per
+//         parity [6][Vh] float4 with complex k in word k/2 (channel = spin).
+// A PtcField holds the two parity bases separately, so the solver's
+// single-parity fields are network inputs and outputs without copies.
 //
 // Weights are BF16 (one __nv_bfloat162 per complex weight) in [9][C_out][C_in]
-// per layer; arithmetic is FP32 (packed FFMA2), reductions FP64.
+// per layer; arithmetic is FP32 (packed FFMA2), weight-gradient sums FP64.
 #pragma once
 #include <cuda_bf16.h>
 
@@ -22,8 +37,13 @@
 
 namespace qkx {
 
-constexpr int PTC_NT = 128;  // threads (sites) per block of the layer kernels
+constexpr int PTC_NT = 128;  // threads of the weight-gradient kernel
 constexpr int PTC_TS = 32;   // sites per tile of the weight-gradient kernel
+constexpr int PTC_SB = 64;   // sites per block of the layer kernel (x 3 colour threads)
+
+struct PtcField {
+  void* p[2];  // per parity: BF16 [C/4][3][Vh] uint4, or FP32 [6][Vh] float4 (C = 4)
+};
 
 // neighbour, link and sign of path p at site (par, cb) with coordinates x and
 // lexicographic index s.  Returns the link already daggered for backward paths
@@ -76,17 +96,48 @@ __device__ __forceinline__ void ptc_mv(const Link<float>& U, const float2 v[3], 
   }
 }
 
-// channels c, c+1 (c even) of an activation at site (par, n): 3 float4 words
-__device__ __forceinline__ void ptc_load_pair(const float4* f, int C, int Vh, int par, int n, int c, float2 v0[3],
-                                              float2 v1[3]) {
-  const float4* b = f + ((size_t)par * (3 * C / 2) + (3 * c) / 2) * Vh + n;
-  const float4 q0 = __ldg(b), q1 = __ldg(b + Vh), q2 = __ldg(b + 2 * (size_t)Vh);
-  v0[0] = make_float2(q0.x, q0.y);
-  v0[1] = make_float2(q0.z, q0.w);
-  v0[2] = make_float2(q1.x, q1.y);
-  v1[0] = make_float2(q1.z, q1.w);
-  v1[1] = make_float2(q2.x, q2.y);
-  v1[2] = make_float2(q2.z, q2.w);
+// BF16 pair <-> FP32 pair (the widening is exact: a BF16 is the upper half of an FP32)
+__device__ __forceinline__ float2 ptc_bf2f(uint32_t w) {
+  return make_float2(__uint_as_float(w << 16), __uint_as_float(w & 0xffff0000u));
+}
+__device__ __forceinline__ uint32_t ptc_f2bf(float2 v) {
+  __nv_bfloat162 h = __floats2bfloat162_rn(v.x, v.y);
+  return *reinterpret_cast<uint32_t*>(&h);
+}
+
+// the four channels of group q at site (par, n), all colours: v[channel][colour]
+template <bool F32>
+__device__ __forceinline__ void ptc_load4(const PtcField& f, int Vh, int par, int n, int q, float2 v[4][3]) {
+  if constexpr (F32) {
+    const float4* b = static_cast<const float4*>(f.p[par]) + n;  // C = 4: q = 0
+#pragma unroll
+    for (int w = 0; w < 6; w++) {
+      const float4 x = __ldg(b + (size_t)w * Vh);
+      v[(2 * w) / 3][(2 * w) % 3] = make_float2(x.x, x.y);
+      v[(2 * w + 1) / 3][(2 * w + 1) % 3] = make_float2(x.z, x.w);
+    }
+  } else {
+    const uint4* b = static_cast<const uint4*>(f.p[par]) + (size_t)(3 * q) * Vh + n;
+    const uint4 w0 = __ldg(b), w1 = __ldg(b + Vh), w2 = __ldg(b + 2 * (size_t)Vh);
+    const uint32_t ws[12] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w, w2.x, w2.y, w2.z, w2.w};
+#pragma unroll
+    for (int k = 0; k < 12; k++) v[k / 3][k % 3] = ptc_bf2f(ws[k]);
+  }
+}
+
+// one complex number: channel ch, colour a of site (par, cb)
+template <bool F32>
+__device__ __forceinline__ void ptc_store1(const PtcField& f, int Vh, int par, int cb, int ch, int a, float2 v) {
+  if constexpr (F32) {
+    const int k = ch * 3 + a;  // C = 4
+    float2* b = reinterpret_cast<float2*>(static_cast<float4*>(f.p[par]) + (size_t)(k >> 1) * Vh + cb) + (k & 1);
+    *b = v;
+  } else {
+    const int q = ch >> 2, k = (ch & 3) * 3 + a;
+    uint32_t* b = reinterpret_cast<uint32_t*>(static_cast<uint4*>(f.p[par]) + (size_t)(3 * q + (k >> 2)) * Vh + cb) +
+                  (k & 3);
+    *b = ptc_f2bf(v);
+  }
 }
 
 // acc += w * s (complex), as two packed FMAs: (w.re, w.re) (s.re, s.im) + (-w.im, w.im) (s.im, s.re)
@@ -94,65 +145,72 @@ __device__ __forceinline__ float2 cfma2(float2 wa, float2 wb, float2 s, float2 a
   return __ffma2_rn(wb, make_float2(s.y, s.x), __ffma2_rn(wa, s, acc));
 }
 
-// One PTC layer, one thread per site.  Blocks alternate parities.  The weights
-// are staged in shared memory as the pairs (w.re, w.re), (-w.im, w.im).
-template <int CI, int CO>
-__global__ void __launch_bounds__(PTC_NT) k_ptc_layer(const float4* __restrict__ in, float4* __restrict__ out,
-                                                      const __nv_bfloat162* __restrict__ w, GaugeF32x12 u, Geom g) {
-  __shared__ float4 sw[9 * CO * CI];
-  for (int i = threadIdx.x; i < 9 * CO * CI; i += PTC_NT) {
+// One PTC layer on the FP32 pipe.  Each site is split over three colour threads
+// (block PTC_SB x 3): thread (site, a) transports every input channel with row a
+// of the path's link and accumulates the CO outputs of colour a only, so a
+// thread holds CO complex accumulators instead of 3 CO.  Blocks alternate
+// parities when npar = 2; npar = 1 computes parity par0 only.  The weights are
+// staged in dynamic shared memory as the pairs (w.re, w.re), (-w.im, w.im).
+template <int CI, int CO, bool IN32, bool OUT32>
+__global__ void __launch_bounds__(PTC_SB * 3, 3)
+    k_ptc_layer(PtcField in, PtcField out, const __nv_bfloat162* __restrict__ w, GaugeF32x12 u, Geom g, int par0,
+                int npar) {
+  static_assert(CI % 4 == 0 && CO % 4 == 0 && (!IN32 || CI == 4) && (!OUT32 || CO == 4), "widths");
+  extern __shared__ float4 ptc_sw[];  // [9][CO][CI]
+  const int tid = threadIdx.y * PTC_SB + threadIdx.x;
+  for (int i = tid; i < 9 * CO * CI; i += PTC_SB * 3) {
     const float2 f = __bfloat1622float2(w[i]);
-    sw[i] = make_float4(f.x, f.x, -f.y, f.y);
+    ptc_sw[i] = make_float4(f.x, f.x, -f.y, f.y);
   }
   __syncthreads();
-  const int par = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * PTC_NT + threadIdx.x;
+  const int par = npar == 2 ? (blockIdx.x & 1) : par0;
+  const int sb = npar == 2 ? (blockIdx.x >> 1) : blockIdx.x;
+  const int cb = sb * PTC_SB + threadIdx.x, a = threadIdx.y;
   if (cb >= g.Vh) return;
   int x[4];
   cb_coords(g, cb, par, x);
   const int s = x[0] + g.L[0] * (x[1] + g.L[1] * (x[2] + g.L[2] * x[3]));
-  float2 acc[CO][3];
+  float2 acc[CO];
 #pragma unroll
-  for (int c = 0; c < CO; c++)
-#pragma unroll
-    for (int a = 0; a < 3; a++) acc[c][a] = make_float2(0.f, 0.f);
+  for (int c = 0; c < CO; c++) acc[c] = make_float2(0.f, 0.f);
 #pragma unroll 1
   for (int p = 0; p < 9; p++) {
     Link<float> U;
     const PtcHop h = ptc_hop(u, g, par, cb, x, s, p, U);
+    // row a of the link
+    Cx<float> ur[3];
+#pragma unroll
+    for (int b = 0; b < 3; b++) ur[b] = a == 0 ? U.m[0][b] : (a == 1 ? U.m[1][b] : U.m[2][b]);
 #pragma unroll 1
-    for (int cp = 0; cp < CI; cp += 2) {
-      float2 v0[3], v1[3], s0[3], s1[3];
-      ptc_load_pair(in, CI, g.Vh, h.npar, h.n, cp, v0, v1);
-      if (p == 0) {
+    for (int q = 0; q < CI / 4; q++) {
+      float2 v[4][3], t[4];
+      ptc_load4<IN32>(in, g.Vh, h.npar, h.n, q, v);
 #pragma unroll
-        for (int a = 0; a < 3; a++) {
-          s0[a] = v0[a];
-          s1[a] = v1[a];
-        }
-      } else {
-        ptc_mv(U, v0, s0);
-        ptc_mv(U, v1, s1);
-      }
-      const float4* wr = sw + (p * CO) * CI + cp;
+      for (int cl = 0; cl < 4; cl++) {
+        if (p == 0) {
+          t[cl] = a == 0 ? v[cl][0] : (a == 1 ? v[cl][1] : v[cl][2]);
+        } else {
+          float re = 0.f, im = 0.f;
 #pragma unroll
-      for (int c = 0; c < CO; c++) {
-        const float4 w0 = wr[c * CI], w1 = wr[c * CI + 1];
-#pragma unroll
-        for (int a = 0; a < 3; a++) {
-          acc[c][a] = cfma2(make_float2(w0.x, w0.y), make_float2(w0.z, w0.w), s0[a], acc[c][a]);
-          acc[c][a] = cfma2(make_float2(w1.x, w1.y), make_float2(w1.z, w1.w), s1[a], acc[c][a]);
+          for (int b = 0; b < 3; b++) {
+            re = fmaf(ur[b].re, v[cl][b].x, fmaf(-ur[b].im, v[cl][b].y, re));
+            im = fmaf(ur[b].re, v[cl][b].y, fmaf(ur[b].im, v[cl][b].x, im));
+          }
+          t[cl] = make_float2(re, im);
         }
       }
+      const float4* wr = ptc_sw + (p * CO) * CI + 4 * q;
+#pragma unroll
+      for (int c = 0; c < CO; c++)
+#pragma unroll
+        for (int cl = 0; cl < 4; cl++) {
+          const float4 wv = wr[c * CI + cl];
+          acc[c] = cfma2(make_float2(wv.x, wv.y), make_float2(wv.z, wv.w), t[cl], acc[c]);
+        }
     }
   }
-  float4* o = out + (size_t)par * (3 * CO / 2) * g.Vh + cb;
 #pragma unroll
-  for (int q = 0; q < 3 * CO / 2; q++) {
-    const int k0 = 2 * q, k1 = 2 * q + 1;
-    o[(size_t)q * g.Vh] = make_float4(acc[k0 / 3][k0 % 3].x, acc[k0 / 3][k0 % 3].y, acc[k1 / 3][k1 % 3].x,
-                                      acc[k1 / 3][k1 % 3].y);
-  }
+  for (int c = 0; c < CO; c++) ptc_store1<OUT32>(out, g.Vh, par, cb, c, a, acc[c]);
 }
 
 // Weight gradient of one layer: dW[p][c][c'] = sum_{x, colour} gy[x][c] conj((T_p a)[x][c'])
@@ -161,9 +219,9 @@ __global__ void __launch_bounds__(PTC_NT) k_ptc_layer(const float4* __restrict__
 // the tile in shared memory and each thread sums whole entries.  Tile sums are
 // FP32 (PTC_TS * 3 terms), accumulated across tiles in FP64; the block's
 // totals go to part[block][9][CO][CI] for a fixed-order reduction.
-template <int CI, int CO>
-__global__ void __launch_bounds__(PTC_NT) k_ptc_wgrad(const float4* __restrict__ a, const float4* __restrict__ gy,
-                                                      GaugeF32x12 u, Geom g, double2* __restrict__ part) {
+template <int CI, int CO, bool A32, bool G32>
+__global__ void __launch_bounds__(PTC_NT) k_ptc_wgrad(PtcField a, PtcField gy, GaugeF32x12 u, Geom g,
+                                                      double2* __restrict__ part) {
   constexpr int NE = CO * CI;
   constexpr int EPT = (NE + PTC_NT - 1) / PTC_NT;  // entries per thread
   __shared__ float2 sS[PTC_TS][CI][3];
@@ -179,55 +237,56 @@ __global__ void __launch_bounds__(PTC_NT) k_ptc_wgrad(const float4* __restrict__
     const int cb0 = (t % tpp) * PTC_TS;
     __syncthreads();
     // output gradient of the tile
-    for (int i = threadIdx.x; i < PTC_TS * (CO / 2); i += PTC_NT) {
-      const int site = i % PTC_TS, cp = 2 * (i / PTC_TS);
+    for (int i = threadIdx.x; i < PTC_TS * (CO / 4); i += PTC_NT) {
+      const int site = i % PTC_TS, q = i / PTC_TS;
       const int cb = cb0 + site;
-      float2 v0[3], v1[3];
+      float2 v[4][3];
       if (cb < g.Vh) {
-        ptc_load_pair(gy, CO, g.Vh, par, cb, cp, v0, v1);
+        ptc_load4<G32>(gy, g.Vh, par, cb, q, v);
       } else {
 #pragma unroll
-        for (int k = 0; k < 3; k++) v0[k] = v1[k] = make_float2(0.f, 0.f);
+        for (int cl = 0; cl < 4; cl++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) v[cl][k] = make_float2(0.f, 0.f);
       }
 #pragma unroll
-      for (int k = 0; k < 3; k++) {
-        sG[site][cp][k] = v0[k];
-        sG[site][cp + 1][k] = v1[k];
-      }
+      for (int cl = 0; cl < 4; cl++)
+#pragma unroll
+        for (int k = 0; k < 3; k++) sG[site][4 * q + cl][k] = v[cl][k];
     }
 #pragma unroll 1
     for (int p = 0; p < 9; p++) {
-      for (int i = threadIdx.x; i < PTC_TS * (CI / 2); i += PTC_NT) {
-        const int site = i % PTC_TS, cp = 2 * (i / PTC_TS);
+      for (int i = threadIdx.x; i < PTC_TS * (CI / 4); i += PTC_NT) {
+        const int site = i % PTC_TS, q = i / PTC_TS;
         const int cb = cb0 + site;
-        float2 s0[3], s1[3];
+        float2 s[4][3];
         if (cb < g.Vh) {
           int x[4];
           cb_coords(g, cb, par, x);
           const int sl = x[0] + g.L[0] * (x[1] + g.L[1] * (x[2] + g.L[2] * x[3]));
           Link<float> U;
           const PtcHop h = ptc_hop(u, g, par, cb, x, sl, p, U);
-          float2 v0[3], v1[3];
-          ptc_load_pair(a, CI, g.Vh, h.npar, h.n, cp, v0, v1);
-          if (p == 0) {
+          float2 v[4][3];
+          ptc_load4<A32>(a, g.Vh, h.npar, h.n, q, v);
 #pragma unroll
-            for (int k = 0; k < 3; k++) {
-              s0[k] = v0[k];
-              s1[k] = v1[k];
+          for (int cl = 0; cl < 4; cl++) {
+            if (p == 0) {
+#pragma unroll
+              for (int k = 0; k < 3; k++) s[cl][k] = v[cl][k];
+            } else {
+              ptc_mv(U, v[cl], s[cl]);
             }
-          } else {
-            ptc_mv(U, v0, s0);
-            ptc_mv(U, v1, s1);
           }
         } else {
 #pragma unroll
-          for (int k = 0; k < 3; k++) s0[k] = s1[k] = make_float2(0.f, 0.f);
+          for (int cl = 0; cl < 4; cl++)
+#pragma unroll
+            for (int k = 0; k < 3; k++) s[cl][k] = make_float2(0.f, 0.f);
         }
 #pragma unroll
-        for (int k = 0; k < 3; k++) {
-          sS[site][cp][k] = s0[k];
-          sS[site][cp + 1][k] = s1[k];
-        }
+        for (int cl = 0; cl < 4; cl++)
+#pragma unroll
+          for (int k = 0; k < 3; k++) sS[site][4 * q + cl][k] = s[cl][k];
       }
       __syncthreads();
 #pragma unroll

@@ -119,17 +119,17 @@ struct __align__(16) TcSmem {
   uint32_t tmem;
 };
 
-// One 16 -> 16 PTC layer on the tensor cores.  Blocks alternate parities; 128
-// threads (4 warps) per block, one site each.  err (if not null) receives a
-// non-zero code when a wait timed out.
-__global__ void __launch_bounds__(TC_M) k_ptc_layer_tc(const float4* __restrict__ in, float4* __restrict__ out,
-                                                       const __nv_bfloat162* __restrict__ w, GaugeF32x12 u, Geom g,
-                                                       int* err) {
+// One 16 -> 16 PTC layer on the tensor cores, BF16 activations in and out.  Blocks
+// alternate parities when npar = 2 (npar = 1: parity par0 only); 128 threads (4
+// warps) per block, one site each.  err (if not null) receives a non-zero code
+// when a wait timed out.
+__global__ void __launch_bounds__(TC_M) k_ptc_layer_tc(PtcField in, PtcField out, const __nv_bfloat162* __restrict__ w,
+                                                       GaugeF32x12 u, Geom g, int par0, int npar, int* err) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   TcSmem& sm = *reinterpret_cast<TcSmem*>(tc_raw);
   const int tid = threadIdx.x, warp = tid >> 5;
-  const int par = blockIdx.x & 1;
-  const int cb = (blockIdx.x >> 1) * TC_M + tid;
+  const int par = npar == 2 ? (blockIdx.x & 1) : par0;
+  const int cb = (npar == 2 ? (blockIdx.x >> 1) : blockIdx.x) * TC_M + tid;
   const bool valid = cb < g.Vh;
 
   // B: real 2x2 blocks of W[p][c][c'] at (n = 2c + i, k = 2c' + j), canonical K-major
@@ -175,25 +175,23 @@ __global__ void __launch_bounds__(TC_M) k_ptc_layer_tc(const float4* __restrict_
 #pragma unroll 1
     for (int c4 = 0; c4 < 16; c4 += 4) {  // four channels = one 16-byte K group
       float2 t[4][3];
+      if (valid) {
+        float2 v[4][3];
+        ptc_load4<false>(in, g.Vh, h.npar, h.n, c4 / 4, v);
 #pragma unroll
-      for (int q = 0; q < 2; q++) {
-        float2 v0[3], v1[3];
-        if (valid) {
-          ptc_load_pair(in, 16, g.Vh, h.npar, h.n, c4 + 2 * q, v0, v1);
+        for (int cl = 0; cl < 4; cl++) {
           if (p == 0) {
 #pragma unroll
-            for (int a = 0; a < 3; a++) {
-              t[2 * q][a] = v0[a];
-              t[2 * q + 1][a] = v1[a];
-            }
+            for (int a = 0; a < 3; a++) t[cl][a] = v[cl][a];
           } else {
-            ptc_mv(U, v0, t[2 * q]);
-            ptc_mv(U, v1, t[2 * q + 1]);
+            ptc_mv(U, v[cl], t[cl]);
           }
-        } else {
-#pragma unroll
-          for (int a = 0; a < 3; a++) t[2 * q][a] = t[2 * q + 1][a] = make_float2(0.f, 0.f);
         }
+      } else {
+#pragma unroll
+        for (int cl = 0; cl < 4; cl++)
+#pragma unroll
+          for (int a = 0; a < 3; a++) t[cl][a] = make_float2(0.f, 0.f);
       }
 #pragma unroll
       for (int a = 0; a < 3; a++) {
@@ -235,13 +233,21 @@ __global__ void __launch_bounds__(TC_M) k_ptc_layer_tc(const float4* __restrict_
 #pragma unroll
     for (int a = 0; a < 3; a++) tc_ld32(lane_base + a * TC_N, d[a]);
     if (valid) {
-      float4* o = out + (size_t)par * 24 * g.Vh + cb;
+      // BF16 layout: group q of four channels, word wd holds complex k = 4 wd + j (channel
+      // 4q + k/3, colour k%3) in slot j
+      uint4* o = static_cast<uint4*>(out.p[par]) + cb;
 #pragma unroll
-      for (int q = 0; q < 24; q++) {
-        const int k0 = 2 * q, k1 = 2 * q + 1;  // complex k = c*3 + colour
-        o[(size_t)q * g.Vh] = make_float4(d[k0 % 3][2 * (k0 / 3)], d[k0 % 3][2 * (k0 / 3) + 1], d[k1 % 3][2 * (k1 / 3)],
-                                          d[k1 % 3][2 * (k1 / 3) + 1]);
-      }
+      for (int q = 0; q < 4; q++)
+#pragma unroll
+        for (int wd = 0; wd < 3; wd++) {
+          uint32_t e[4];
+#pragma unroll
+          for (int j = 0; j < 4; j++) {
+            const int k = 4 * wd + j, ch = 4 * q + k / 3, col = k % 3;
+            e[j] = ptc_f2bf(make_float2(d[col][2 * ch], d[col][2 * ch + 1]));
+          }
+          o[(size_t)(3 * q + wd) * g.Vh] = make_uint4(e[0], e[1], e[2], e[3]);
+        }
     }
   } else if (err && tid == 0) {
     atomicExch(err, 1);

@@ -84,3 +84,29 @@ def test_identity_path_only_is_identity(oracle):
         W[off + a * 8 + a, 0] = 1.0
     r = oracle.spinor_gaussian(L, 8)
     assert np.array_equal(oracle.ptc_forward(L, U, ch, W, r), r)
+
+
+def test_bf16_activation_mode(oracle):
+    """The BF16 mode rounds the hidden activations (and only those): the output moves by
+    about a BF16 rounding (2^-9 relative), its hidden inputs are exactly representable in
+    BF16, and a one-layer network (no hidden activation) is unchanged."""
+    U, W = _setup(oracle)
+    r = oracle.spinor_gaussian(L, 8)
+    a = oracle.ptc_forward(L, U, CH, W, r)
+    b = oracle.ptc_forward(L, U, CH, W, r, bf16=True)
+    d = np.linalg.norm(a - b) / np.linalg.norm(a)
+    assert 0 < d < 2.0 ** -7
+    one = [4, 4]
+    W1 = W[:oracle.ptc_nweights(one)]
+    assert np.array_equal(oracle.ptc_forward(L, U, one, W1, r), oracle.ptc_forward(L, U, one, W1, r, bf16=True))
+    # the mode is reset after each call
+    assert np.array_equal(oracle.ptc_forward(L, U, CH, W, r), a)
+    # widths 4 -> 4 -> 4 with an identity first layer: the hidden activation is r rounded to BF16
+    ident = np.zeros((oracle.ptc_nweights([4, 4, 4]), 2))
+    for c in range(4):
+        ident[c * 4 + c, 0] = 1.0                  # layer 0, path 0
+        ident[9 * 16 + c * 4 + c, 0] = 1.0         # layer 1, path 0
+    y = oracle.ptc_forward(L, U, [4, 4, 4], ident, r, bf16=True)
+    bits = y.astype(np.float32).view(np.uint32)
+    assert np.all(bits & 0xFFFF == 0)
+    assert np.abs(y - r).max() <= 2.0 ** -8 * np.abs(r).max()
