@@ -30,7 +30,7 @@ Other workloads (one JSON line each, same --steps/--warmup rules, 1 GPU):
                          12 solves of 4 Gaussian sources, run concurrently
   --workload ptc         the learned preconditioner at 32^3x64: 64 training solves,
                          --ptc-steps Adam steps, then the 12 point sources in one batch by
-                         flexible GCR on the even-odd system, preconditioned by the network
+                         flexible CG on the even-odd system, preconditioned by the network
   --workload contract    the 10 meson and 4 nucleon two-point functions with 33
                          momenta (Q^2 <= 4) from a 32^3x64 propagator in HBM
   --workload dslash      the Dslash alone: the 12-RHS even-odd hop in FP16 and FP32

@@ -1,5 +1,5 @@
 // ptc.cu -- the learned preconditioner: network object, training on
-// (residual, error) pairs from the library's own solves, and the flexible GCR
+// (residual, error) pairs from the library's own solves, and the flexible CG
 // solver that uses it (QKX_SOLVER_GCR_PTC).  No reference counterpart.
 #include <math.h>
 #include <string.h>

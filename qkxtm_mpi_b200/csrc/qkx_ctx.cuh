@@ -154,7 +154,7 @@ void mixed_free(qkx_ctx* c);
 // qkx_invert_batch as one graph launch for all lattices (CG_EO_MIXED, graphs on): 0 done,
 // 1 not applicable, < 0 error; t0 is the batch's start on the steady clock, in seconds
 int invert_batch_graph(qkx_batch_job* jobs, int njobs, const qkx_solver_params* sp, double t0);
-// flexible GCR with the learned preconditioner (ptc.cu)
+// the learned solver: batched even-odd flexible CG preconditioned by the network (ptc.cu)
 int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const double2* const* b, double2* const* x,
                    qkx_solve_info* info);
 void mixed_invalidate(qkx_ctx* c);

@@ -13,7 +13,7 @@ reference's Vector::tm, lib/lattice_util.cpp:1925) unless stated otherwise.
              every job's FP64 true residual as the library reports it, and the
              16^3x32 job's solutions by the oracle
   learned    32^3x64 with the learned preconditioner after a short training run,
-             flexible GCR on two point sources
+             flexible CG on two point sources
 
 Tolerance: 1e-10 on every true residual, as the solves are asked for."""
 import numpy as np
