@@ -105,19 +105,33 @@ int layer(qkx_ctx* c, int ci, int co, PtcField in, bool in32, PtcField out, bool
   return QKX_OK;
 }
 
-// 16 -> 16 layer on the tensor cores (ptc_tc.cuh), BF16 in and out
-int layer_tc(qkx_ctx* c, PtcField in, PtcField out, const __nv_bfloat162* w, int* err) {
-  static bool attr = false;
-  if (!attr) {
-    QKX_CUDA(cudaFuncSetAttribute(k_ptc_layer_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(TcSmem)));
-    attr = true;
-  }
-  const int nb = 2 * ((c->Vh + TC_M - 1) / TC_M);
-  k_ptc_layer_tc<<<nb, TC_M, sizeof(TcSmem), c->st>>>(in, out, w, GaugeF32x12{c->U12f, c->Vh}, c->geom_raw, 0, 2,
-                                                      err);
+// 16 -> co layer on the tensor cores (ptc_tc.cuh): BF16 in, BF16 out or (out32, co = 4) the
+// FP32 spinor layout; npar = 1 computes the output parity par0 only.  The kernel's shared
+// memory (43 KB) is within the default limit.
+template <int CI, int CO, bool I32, bool O32>
+int layer_tc_t(qkx_ctx* c, PtcField in, PtcField out, const __nv_bfloat162* w, int* err, int par0, int npar) {
+  static_assert(sizeof(TcSmem) <= 48 * 1024, "the tensor-core layer's shared memory needs no opt-in");
+  const int nb = npar * ((c->Vh + TC_M - 1) / TC_M);
+  k_ptc_layer_tc<CI, CO, I32, O32><<<nb, TC_M, sizeof(TcSmem), c->st>>>(
+      in, out, w, GaugeF32x12{c->U12f, c->Vh}, c->geom_raw, par0, npar, err);
   counted(c);
   QKX_CUDA(cudaGetLastError());
   return QKX_OK;
+}
+// whether a layer has a tensor-core form: 16 channels on one side, the other 4 or 16
+inline bool tc_layer(int ci, int co) { return (ci == 16 && (co == 16 || co == 4)) || (ci == 4 && co == 16); }
+int layer_tc(qkx_ctx* c, int ci, int co, bool in32, bool out32, PtcField in, PtcField out, const __nv_bfloat162* w,
+             int* err, int par0 = 0, int npar = 2) {
+  if (ci == 16 && co == 16 && !in32 && !out32) return layer_tc_t<16, 16, false, false>(c, in, out, w, err, par0, npar);
+  if (ci == 16 && co == 4 && !in32) {
+    if (out32) return layer_tc_t<16, 4, false, true>(c, in, out, w, err, par0, npar);
+    return layer_tc_t<16, 4, false, false>(c, in, out, w, err, par0, npar);
+  }
+  if (ci == 4 && co == 16 && !out32) {
+    if (in32) return layer_tc_t<4, 16, true, false>(c, in, out, w, err, par0, npar);
+    return layer_tc_t<4, 16, false, false>(c, in, out, w, err, par0, npar);
+  }
+  return bad("tensor-core layer widths");
 }
 
 int wgrad(qkx_ctx* c, int ci, int co, PtcField a, bool a32, PtcField gy, bool g32, double2* part, int nblocks) {
@@ -285,7 +299,8 @@ int refresh_backward_weights(qkx_ptc* n) {
 }
 
 // out = N(in) on FP32 4-channel fields; the hidden activations stay in hid[1..nl-1]
-// (BF16) for the backward pass.  With tc the 16 -> 16 layers run on the tensor cores.
+// (BF16) for the backward pass.  With tc the layers with 16 channels on one side (4 or 16 on the
+// other) run on the tensor cores.
 // out_npar = 1 computes the output on parity out_par0 only (the even-odd solver reads
 // the even sites of N applied to an even-site input).
 int forward(qkx_ptc* n, PtcField in, PtcField out, bool tc = false, int out_par0 = 0, int out_npar = 2) {
@@ -295,8 +310,9 @@ int forward(qkx_ptc* n, PtcField in, PtcField out, bool tc = false, int out_par0
   for (int l = 0; l < n->nl; l++) {
     const bool last = l == n->nl - 1;
     const PtcField dst = last ? out : bf_field(n->hid[l + 1], n->ch[l + 1], Vh);
-    if (tc && !s32 && !last && n->ch[l] == 16 && n->ch[l + 1] == 16)
-      QKX_TRY(layer_tc(n->c, src, dst, n->wb + n->woff[l], n->tc_err));
+    if (tc && tc_layer(n->ch[l], n->ch[l + 1]))
+      QKX_TRY(layer_tc(n->c, n->ch[l], n->ch[l + 1], s32, last, src, dst, n->wb + n->woff[l], n->tc_err,
+                       last ? out_par0 : 0, last ? out_npar : 2));
     else
       QKX_TRY(layer(n->c, n->ch[l], n->ch[l + 1], src, s32, dst, last, n->wb + n->woff[l], last ? out_par0 : 0,
                     last ? out_npar : 2));
@@ -322,7 +338,7 @@ int check_tc(qkx_ptc* n) {
 
 // dL/dW^* of every layer into n->grad, from gy = dL/dy^* at the output (FP32) and the
 // activations of the last forward(in).  The activation gradients between layers are
-// BF16, like the activations; with tc the 16 -> 16 ones run on the tensor cores.
+// BF16, like the activations; with tc the layers with a tensor-core form run there.
 int backward(qkx_ptc* n, PtcField in, PtcField gy, bool tc = false) {
   qkx_ctx* c = n->c;
   const int Vh = c->Vh;
@@ -339,8 +355,8 @@ int backward(qkx_ptc* n, PtcField in, PtcField gy, bool tc = false) {
     QKX_CUDA(cudaGetLastError());
     if (l == 0) break;
     const PtcField h = bf_field(n->gb[slot], ci, Vh);
-    if (tc && !g32 && ci == 16 && co == 16)
-      QKX_TRY(layer_tc(c, g, h, n->wt + n->woff[l], n->tc_err));
+    if (tc && tc_layer(co, ci))
+      QKX_TRY(layer_tc(c, co, ci, g32, false, g, h, n->wt + n->woff[l], n->tc_err));
     else
       QKX_TRY(layer(c, co, ci, g, g32, h, false, n->wt + n->woff[l]));
     g = h;
@@ -525,8 +541,9 @@ int adjoint(qkx_ptc* n, PtcField in, PtcField out, bool tc, int out_par0, int ou
     const int ci = n->ch[l + 1], co = n->ch[l];  // the adjoint of layer l maps ch[l+1] -> ch[l]
     const bool last = l == 0;
     const PtcField dst = last ? out : bf_field(n->gb[slot], co, Vh);
-    if (tc && !s32 && !last && ci == 16 && co == 16)
-      QKX_TRY(layer_tc(n->c, src, dst, n->wt + n->woff[l], n->tc_err));
+    if (tc && tc_layer(ci, co))
+      QKX_TRY(layer_tc(n->c, ci, co, s32, last, src, dst, n->wt + n->woff[l], n->tc_err, last ? out_par0 : 0,
+                       last ? out_npar : 2));
     else
       QKX_TRY(layer(n->c, ci, co, src, s32, dst, last, n->wt + n->woff[l], last ? out_par0 : 0,
                     last ? out_npar : 2));
@@ -718,9 +735,11 @@ int invert_gcr_ptc(qkx_ctx* c, const qkx_solver_params* sp, int nrhs, const doub
       if (!act[r]) continue;
       rn0[r] = h[(size_t)r * 8];
       rz[r] = h[(size_t)r * 8 + 2];
-      // the FP32 inner solve: |r| down by 1e-5, or by what the outer target still needs
+      // the FP32 inner solve: |r| down by 1e-6 (the recursive FP32 residual keeps falling past
+      // that; the pass's FP64 residual then says how far the true one went), or by what the
+      // outer target still needs
       const double rel = sqrt(r2[r] / b2[r]);
-      const double t = std::max(0.5 * sp->tol / rel, 1e-5);
+      const double t = std::max(0.5 * sp->tol / rel, 1e-6);
       tgt[r] = t * t * rn0[r];
     }
     for (;;) {

@@ -14,8 +14,8 @@
 // with it; the weights must act on a channel index and leave colour to the
 // transports.  A spin-colour spinor is therefore 4 channels of colour vectors,
 // and a hidden width of 16 channels is 16 colour vectors (48 complex numbers a
-// site): the gauge-covariant form of a 12 -> 16 -> 16 -> 12 complex network is
-// 4 -> 16 -> 16 -> 4 here.
+// site): the gauge-covariant form of a 12 -> 16 -> 16 -> 12 complex network has
+// 4 spin channels in and out and 16 hidden, 4 -> 16 -> ... -> 16 -> 4 here.
 //
 // Activation fields.  Channel c, colour b of a site is complex number
 // k = c*3 + b; the four channels of group q = c/4 are 12 complex numbers in
@@ -181,10 +181,27 @@ __global__ void __launch_bounds__(PTC_SB * 3, 3)
     Cx<float> ur[3];
 #pragma unroll
     for (int b = 0; b < 3; b++) ur[b] = a == 0 ? U.m[0][b] : (a == 1 ? U.m[1][b] : U.m[2][b]);
-#pragma unroll 1
+    // with few outputs the registers allow every input group's loads in flight at once
+    constexpr bool PF = !IN32 && CO <= 8;
+    uint4 raw[PF ? CI / 4 : 1][3];
+    if constexpr (PF) {
+#pragma unroll
+      for (int q = 0; q < CI / 4; q++)
+#pragma unroll
+        for (int k = 0; k < 3; k++)
+          raw[q][k] = __ldg(static_cast<const uint4*>(in.p[h.npar]) + (size_t)(3 * q + k) * g.Vh + h.n);
+    }
+#pragma unroll(PF ? CI / 4 : 1)
     for (int q = 0; q < CI / 4; q++) {
       float2 v[4][3], t[4];
-      ptc_load4<IN32>(in, g.Vh, h.npar, h.n, q, v);
+      if constexpr (PF) {
+        const uint32_t ws[12] = {raw[q][0].x, raw[q][0].y, raw[q][0].z, raw[q][0].w, raw[q][1].x, raw[q][1].y,
+                                 raw[q][1].z, raw[q][1].w, raw[q][2].x, raw[q][2].y, raw[q][2].z, raw[q][2].w};
+#pragma unroll
+        for (int k = 0; k < 12; k++) v[k / 3][k % 3] = ptc_bf2f(ws[k]);
+      } else {
+        ptc_load4<IN32>(in, g.Vh, h.npar, h.n, q, v);
+      }
 #pragma unroll
       for (int cl = 0; cl < 4; cl++) {
         if (p == 0) {
