@@ -1544,6 +1544,13 @@ static int batch_graph_t(std::vector<BatchGroup>& groups, qkx_batch_job* jobs, c
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t start = nullptr;
   QKX_CUDA(cudaGraphCreate(&top, 0));
+  // Each lattice's branch is captured on a stream of its own priority, the smallest lattice the
+  // highest, and the graph runs its kernel nodes at those priorities: the branches still share the
+  // SMs, but the small lattices' blocks go first, so their jobs finish early instead of all jobs
+  // finishing together at the end of the largest one.
+  int prio_least = 0, prio_greatest = 0;
+  QKX_CUDA(cudaDeviceGetStreamPriorityRange(&prio_least, &prio_greatest));
+  std::vector<cudaStream_t> pstreams(groups.size(), nullptr);
   int rc = QKX_OK;
   for (size_t j = 0; j < groups.size() && rc == QKX_OK; j++) {
     MixedSolve<P>& s = *solves[j];
@@ -1553,6 +1560,14 @@ static int batch_graph_t(std::vector<BatchGroup>& groups, qkx_batch_job* jobs, c
       rc = QKX_ERR_CUDA;
       break;
     }
+    const int prio = std::max(prio_greatest, prio_least - (int)j);  // groups come largest first
+    if (cudaStreamCreateWithPriority(&pstreams[j], cudaStreamNonBlocking, prio) != cudaSuccess) {
+      set_error("batch: cudaStreamCreateWithPriority failed");
+      rc = QKX_ERR_CUDA;
+      break;
+    }
+    cudaStream_t own = g.c->st;
+    g.c->st = pstreams[j];  // the capture records the branch on the prioritised stream
     long long kt = 0, ko = 0, ki = 0;
     rc = s.loop_graph(
         top, &kt, &ko, &ki, [&]() { return s.setup(); },
@@ -1561,11 +1576,14 @@ static int batch_graph_t(std::vector<BatchGroup>& groups, qkx_batch_job* jobs, c
           QKX_CUDA(cudaEventRecordWithFlags(g.done, g.c->st, cudaEventRecordExternal));
           return QKX_OK;
         });
+    g.c->st = own;
     s.kcount[0] = kt;
     s.kcount[1] = ko;
     s.kcount[2] = ki;
   }
-  if (rc == QKX_OK && cudaGraphInstantiate(&exec, top, 0) != cudaSuccess) {
+  for (cudaStream_t ps : pstreams)
+    if (ps) cudaStreamDestroy(ps);
+  if (rc == QKX_OK && cudaGraphInstantiate(&exec, top, cudaGraphInstantiateFlagUseNodePriority) != cudaSuccess) {
     set_error("batch: instantiating the graph failed: %s", cudaGetErrorString(cudaGetLastError()));
     rc = QKX_ERR_CUDA;
   }
