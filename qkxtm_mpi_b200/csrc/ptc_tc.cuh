@@ -139,7 +139,7 @@ struct __align__(16) TcSmem {
 // par0 only); 128 threads (4 warps) per block, one site each.  err (if not null) receives a
 // non-zero code when a wait timed out.
 template <int CI, int CO, bool IN32, bool OUT32>
-__global__ void __launch_bounds__(TC_M) k_ptc_layer_tc(PtcField in, PtcField out, const __nv_bfloat162* __restrict__ w,
+__global__ void __launch_bounds__(TC_M, 5) k_ptc_layer_tc(PtcField in, PtcField out, const __nv_bfloat162* __restrict__ w,
                                                        GaugeF32x12 u, Geom g, int par0, int npar, int* err) {
   static_assert((CI == 16 && !IN32) || CI == 4, "input width");
   static_assert((CO == 16 && !OUT32) || CO == 4, "output width");
