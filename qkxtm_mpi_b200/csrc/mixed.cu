@@ -163,34 +163,6 @@ static void bfield_free(BField& f) {
 constexpr int MX_NT = 256;
 constexpr int MX_GRID = 148 * 2;  // blocks per RHS for the streaming kernels
 
-// r_s -= alpha A p and |r_s|^2 partials, one RHS per blockIdx.y.  (x_s += alpha p is done by
-// k_mx_update_p, which reads p anyway: one p read less per site and RHS.)
-template <class SP, class AC, typename R>
-__global__ void __launch_bounds__(MX_NT) k_mx_update_r(SP Ap, AC rs, const CgScalars* sc, double* part) {
-  const int r = blockIdx.y;
-  double* slot = part + (size_t)r * gridDim.x + blockIdx.x;
-  if (!sc->active[r]) {
-    if (threadIdx.x == 0) *slot = 0.0;
-    return;
-  }
-  const R alpha = R(sc->alpha[r]);
-  const SP Apr = Ap.shift(r);
-  const AC rr = rs.shift(r);
-  double acc = 0.0;
-  for (int cb = blockIdx.x * MX_NT + threadIdx.x; cb < Ap.Vh; cb += gridDim.x * MX_NT) {
-    Spinor<R> av = Apr.load(0, cb), rv = rr.load(0, cb);
-#pragma unroll
-    for (int k = 0; k < 12; k++) {
-      Cx<R>& Q = rv.c[k / 3][k % 3];
-      Q = Q - alpha * av.c[k / 3][k % 3];
-      acc += double(Q.re) * double(Q.re) + double(Q.im) * double(Q.im);
-    }
-    rr.store(0, cb, rv);
-  }
-  double s = block_sum<MX_NT>(acc);
-  if (threadIdx.x == 0) *slot = s;
-}
-
 // x_s += alpha p, then p = r_s + beta p (alpha of this iteration, beta from the new r_s)
 template <class SP, class AC, typename R>
 __global__ void __launch_bounds__(MX_NT) k_mx_update_p(SP p, AC xs, AC rs, const CgScalars* sc) {

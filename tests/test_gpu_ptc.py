@@ -184,3 +184,26 @@ def test_ptc_argument_checks(qkx, setup):
     with pytest.raises(qkx.QkxError) as e:
         qkx.Ptc(lat, (8, 16, 4))
     assert e.value.code == qkx.ERR_INVALID
+
+
+def test_learned_solver_per_rhs_masses_and_zero_source(qkx, oracle, setup):
+    """The batched learned solver takes a twisted mass per right-hand side (qkx_solver_params.mu)
+    and returns x = 0 for a zero source, the others to 1e-10 by the oracle."""
+    import ctypes as C
+    lat, U = setup
+    mus = [0.004, 0.01, 0.02]
+    bs = [oracle.spinor_gaussian(L, 80), np.zeros((oracle.volume(L), 4, 3, 2)), oracle.spinor_gaussian(L, 81)]
+    xs = [np.empty_like(b) for b in bs]
+    n = len(bs)
+    arr = (C.c_double * n)(*mus)
+    sp = qkx.SolverParams(qkx.SOLVER_GCR_PTC, qkx.PREC_HALF, 1e-10, 10000, 0.0, 1,
+                          C.cast(arr, C.POINTER(C.c_double)), None)
+    info = qkx.SolveInfo()
+    bp = (C.c_void_p * n)(*[b.ctypes.data for b in bs])
+    xp = (C.c_void_p * n)(*[x.ctypes.data for x in xs])
+    qkx.check(qkx.lib().qkx_invert(lat.ctx, C.byref(sp), n, bp, xp, C.byref(info)))
+    assert info.converged == 1
+    assert not xs[1].any()
+    for mu, b, x in ((mus[0], bs[0], xs[0]), (mus[2], bs[2], xs[2])):
+        r = b - oracle.apply("tm", L, U, x, KAPPA, mu)
+        assert np.linalg.norm(r) / np.linalg.norm(b) <= 1e-10
