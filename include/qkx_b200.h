@@ -268,8 +268,9 @@ QKX_API int qkx_invert_dev(qkx_ctx* ctx, const qkx_solver_params* sp, int nrhs, 
  * the job's).  For QKX_SOLVER_CG_EO_MIXED with use_graphs, the jobs of a
  * context are merged into one batch (each right-hand side keeps its twisted
  * mass) and every context's whole solve is one branch of a single CUDA graph:
- * all lattices run from one launch and share the GPU, largest lattice first;
- * a job's latency is when its lattice's branch ended, and its info is its
+ * all lattices run from one launch and share the GPU, each branch at a stream
+ * priority that grows as the lattice's volume falls (small lattices finish
+ * first); a job's latency is when its lattice's branch ended, and its info is its
  * lattice's (true_residual the worst of the job's own right-hand sides; the
  * phase times are 0).  Otherwise the jobs of a context run in order on one
  * host thread and different contexts on different threads, so their kernels
