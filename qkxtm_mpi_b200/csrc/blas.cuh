@@ -20,7 +20,7 @@ struct CgScalars {
   double pAp[MAX_RHS];
   double alpha[MAX_RHS];
   double beta[MAX_RHS];
-  double stop[MAX_RHS];
+  double stop[MAX_RHS];   // FP64 true residual^2 at which the RHS has converged ((0.9 tol)^2 |b|^2)
   int active[MAX_RHS];   // 1 while the RHS still iterates
   int iters[MAX_RHS];
   double aux[MAX_RHS];   // per-RHS results of the batched FP64 residual steps

@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(MAX_RHS) k_ctl_start(CgScalars* sc, MxCtl* ctl
   if (i < ctl->nrhs) {
     const double bn = sc->aux[i], rh = sc->aux2[i], r2 = sc->r2[i];
     ctl->bnorm2[i] = bn;
+    sc->stop[i] = ctl->target2 * bn;
     ctl->best[i] = rh;
     ctl->r2ru[i] = r2;
     ctl->ratio[i] = r2 > 0 ? rh / r2 : 1.0;
@@ -377,6 +378,14 @@ __global__ void __launch_bounds__(MAX_RHS) k_ctl_start(CgScalars* sc, MxCtl* ctl
     ctl->ru_ns = 0;
     cudaGraphSetConditional(h_outer, any ? 1u : 0u);
   }
+}
+
+// in a reliable update, once the FP64 true residuals are summed (aux): a RHS whose residual meets
+// the tolerance stops there, before the FP32 Mh^+ rhat of the update, which then skips it.  The
+// decisions after the update apply the same test to the same numbers and stop it too.
+__global__ void __launch_bounds__(MAX_RHS) k_mx_stop_converged(CgScalars* sc, int nrhs) {
+  const int i = threadIdx.x;
+  if (i < nrhs && sc->active[i] && sc->aux[i] <= sc->stop[i]) sc->active[i] = 0;
 }
 
 // first node of every outer pass: the inner loop runs at least once
@@ -1092,7 +1101,8 @@ struct MixedSolve {
   }
 
   // reliable update of the active RHS: x64 += x_s (x_s = 0); the FP64 true residual
-  // |rhat|^2 -> aux; the residual the sloppy CG restarts from, Mh^+ rhat, with its norm -> aux2
+  // |rhat|^2 -> aux, after which the RHS that meet the tolerance stop; for the others the residual
+  // the sloppy CG restarts from, Mh^+ rhat, with its norm -> aux2
   int reliable_update() {
     k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
     counted(c);
@@ -1108,12 +1118,16 @@ struct MixedSolve {
                               true));
       k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbz, FIN_AUX, c->sc);
       counted(c);
+      k_mx_stop_converged<<<1, MAX_RHS, 0, c->st>>>(c->sc, nrhs);
+      counted(c);
       QKX_TRY(normal_residual_from32(c, nrhs, FA::acc(m->rs, 0, Vh), &nb));
     } else {
       QKX_TRY(schur64_g5_batch(c, nrhs, +1.0, m->x64, m->z64, nullptr));
       k_mx_sub_norm<<<bg2, MX_NT, 0, c->st>>>(B64(m->g5bh, 0, Vh), B64(m->z64, 0, Vh), c->sc->active, m->part);
       counted(c);
       k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, MX_GRID, FIN_AUX, c->sc);
+      counted(c);
+      k_mx_stop_converged<<<1, MAX_RHS, 0, c->st>>>(c->sc, nrhs);
       counted(c);
       QKX_TRY(schur64_g5_batch(c, nrhs, -1.0, m->z64, m->r64, m->part, &nb));
     }
@@ -1231,8 +1245,10 @@ struct MixedSolve {
       ratio[i] = sh->r2[i] > 0 ? sh->aux2[i] / sh->r2[i] : 1.0;  // ||rhat||^2 / ||Mh^+ rhat||^2 at x = 0
       if (bnorm2[i] == 0.0 || sh->r2[i] == 0.0) active[i] = 0;
       sh->active[i] = active[i];
+      sh->stop[i] = target * target * bnorm2[i];
     }
     QKX_CUDA(cudaMemcpyAsync(c->sc->active, sh->active, sizeof(int) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
+    QKX_CUDA(cudaMemcpyAsync(c->sc->stop, sh->stop, sizeof(double) * MAX_RHS, cudaMemcpyHostToDevice, c->st));
 
     // --- graph of one inner iteration
     if (prof && m->gev.size() < 8) {
