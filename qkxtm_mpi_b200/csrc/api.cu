@@ -332,6 +332,9 @@ int hop64_batch(qkx_ctx* c, int epi, int nrhs, SpinorF64 in, SpinorF64 out, Spin
     case EPI_XPAY_TWINV:
       return hop64_batch_t<EPI_XPAY_TWINV>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active,
                                            norm_part, nblk);
+    case EPI_XPAY_TWINV_RES:
+      return hop64_batch_t<EPI_XPAY_TWINV_RES>(c, nrhs, in, out, x, out_parity, a, csign, cvec, svec, active,
+                                               norm_part, nblk);
   }
   return invalid("epilogue");
 }

@@ -33,6 +33,8 @@ enum Epilogue {
   EPI_XPAY_G5_CGR = 7, // o = g5 (a D psi + x + i c g5 x) is not stored: the CG residual of the batch
                        // takes it, r -= alpha o, and |r|^2 goes to the norm partials (multi-RHS
                        // kernels of the mixed solver only; r is racc32, or racc64 for FP64 sloppy)
+  EPI_XPAY_TWINV_RES = 8,  // as EPI_XPAY_TWINV, and |v - (out + i c g5 out)|^2 to the norm partials: with
+                           // x = b_o, a = kappa the odd half of ||b - M x||^2 (hop_c3_kernel only)
 };
 
 // extra operands of EPI_XPAY_G5_RES / EPI_XPAY_RES: w, and the FP32 field the residual

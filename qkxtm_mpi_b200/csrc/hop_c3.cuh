@@ -101,10 +101,19 @@ __device__ __forceinline__ double c3_epilogue(const HopArgs<SP, GaugeF64x18>& A,
     Spin4<double> v;
 #pragma unroll
     for (int sp = 0; sp < 4; sp++) v.s[sp] = ldc(xb + (size_t)(sp * 3 + a) * Vh);
-    if constexpr (EPI == EPI_XPAY_TWINV) {
+    if constexpr (EPI == EPI_XPAY_TWINV || EPI == EPI_XPAY_TWINV_RES) {
 #pragma unroll
       for (int sp = 0; sp < 4; sp++) v.s[sp] = A.a * acc.s[sp] + v.s[sp];
       o = twist_inv4<B>(v, c, sc);
+      if constexpr (EPI == EPI_XPAY_TWINV_RES) {
+        // the residual of the reconstructed sites, v - A o with A = 1 + i c g5
+        const Spin4<double> g5o = gamma5_4<B>(o);
+#pragma unroll
+        for (int sp = 0; sp < 4; sp++) {
+          const Cx<double> z = v.s[sp] - (o.s[sp] + c * phase<1>(g5o.s[sp]));
+          nrm += z.re * z.re + z.im * z.im;
+        }
+      }
     } else {
       const Spin4<double> g5v = gamma5_4<B>(v);
 #pragma unroll
@@ -133,7 +142,7 @@ __device__ __forceinline__ double c3_epilogue(const HopArgs<SP, GaugeF64x18>& A,
 #pragma unroll
     for (int sp = 0; sp < 4; sp++) {
       ob[(size_t)(sp * 3 + a) * Vh] = make_double2(o.s[sp].re, o.s[sp].im);
-      nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
+      if constexpr (EPI != EPI_XPAY_TWINV_RES) nrm += o.s[sp].re * o.s[sp].re + o.s[sp].im * o.s[sp].im;
     }
   }
   return nrm;

@@ -1397,16 +1397,20 @@ struct MixedSolve {
       k_mx_fold<AC, R><<<cg2, 256, 0, c->st>>>(FA::acc(m->xs, 0, Vh), B64(m->x64, 0, Vh), c->sc->active);
       counted(c);
     }
-    // x_o = A^-1 (b_o + k D_oe x_e) into t64
-    QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k, 1.0,
-                        m->cvec, m->svec, c->sc->active, nullptr, nullptr));
-    // ||b - M x||^2 on the full lattice (x: even half in x64, odd half in t64), summed in FP64 by the
-    // hop's epilogue; nothing is stored
-    int nbr = 0;
+    // x_o = A^-1 (b_o + k D_oe x_e) into t64; the same kernel sums the odd half of ||b - M x||^2,
+    // |v - A_oo x_o|^2 with v = b_o + k D_oe x_e, from the D_oe x_e it has just computed
+    int nbo = 0;
+    QKX_TRY(hop64_batch(c, EPI_XPAY_TWINV_RES, nrhs, B64(m->x64, 0, Vh), B64(m->t64, 1, Vh), B64(m->bO, 1, Vh), 1, k,
+                        1.0, m->cvec, m->svec, c->sc->active, m->part, &nbo));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbo, FIN_AUX, c->sc);
+    counted(c);
+    // the even half, ||b_e - (A_ee x_e - k D_eo x_o)||^2 (x: even half in x64, odd half in t64),
+    // summed in FP64 by the hop's epilogue; nothing is stored
+    int nbe = 0;
     QKX_TRY(hop64_batch_res(c, nrhs, B64full(m->x64, m->t64, Vh), B64full(m->x64, m->t64, Vh),
-                            B64full(m->bE, m->bO, Vh), SpinorF32{nullptr, nullptr, Vh}, -1, -k, 1.0, m->cvec,
-                            c->sc->active, m->part, &nbr, false));
-    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbr, FIN_AUX, c->sc);
+                            B64full(m->bE, m->bO, Vh), SpinorF32{nullptr, nullptr, Vh}, 0, -k, 1.0, m->cvec,
+                            c->sc->active, m->part, &nbe, false));
+    k_mx_finalize<<<nrhs, 256, 0, c->st>>>(m->part, nbe, FIN_AUX_ADD, c->sc);
     counted(c);
     QKX_CUDA(cudaGetLastError());
     for (int i = 0; i < nrhs; i++) {
